@@ -1,0 +1,356 @@
+"""Benchmark: BN254-Fr forward NTT of 2^24 elements on B200, one JSON line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl zntt|reference] [--log-n L]
+
+A step is one forward transform (zig-ntt nttWithTwiddles semantics,
+libs/ntt/src/root.zig:148-175) of 2^24 seeded uniform BN254-Fr elements with
+the twiddle table resident on the device.  `value` is elements/s over all
+ranks with the input already in HBM (512 MiB per vector, larger than the
+126 MB L2, so no flush is needed between steps).  `e2e` is the same metric
+through the C ABI's host-buffer entry point zntt_ntt_with_twiddles, whose
+timed call includes the host->device copy of the input from pinned memory and
+the device->host copy of the result.  Under torchrun every rank transforms its
+own vector (independent objects: weak scaling, no collective on the data
+path); the time is the max over ranks.
+
+`--impl reference` times the CPU restatement of zig-ntt (oracle/) on all host
+cores instead: zig-ntt has no GPU path and its toolchain (Zig 0.16) is not
+available, so the reference arm is the oracle port with the reference's
+fork-join pool semantics (libs/parallel/src/root.zig:45-79).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+IMAD_PER_MODMUL = 264  # multiply-class instructions in one 8x32-bit CIOS product
+METRIC = "BN254-Fr NTT elems/s at 2^24"
+
+
+def load_package():
+    name = "zig_algebra_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg = os.path.join(ROOT, "zig-algebra_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def read_traffic(log_n: int):
+    """DRAM bytes per pass launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", f"ntt_pass_bn254_fr_2p{log_n}.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        return json.load(open(path)), "measured"
+    return {"hbm_gbs": 6650.0}, "fallback"
+
+
+# --- CPU baseline (the oracle port) ------------------------------------------------------
+
+def cpu_oracle(native: bool = True):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    lib = None
+    if native:
+        try:
+            lib = O.load(O.build(native=True))
+        except Exception:  # noqa: BLE001 -- fall back to the portable build of the checker
+            lib = None
+    if lib is None:
+        O.load()
+        lib = O.load(os.path.join(ROOT, "oracle", "liboracle.so"))
+    return O, lib
+
+
+def cpu_transform_seconds(O, lib, data, log_n, stages, workers):
+    """One in-place oracle nttWithTwiddles over `data`, fork-join over `workers` threads."""
+    ptrs = (O._U64P * len(stages))()
+    lens = (ctypes.c_size_t * len(stages))()
+    for s, a in enumerate(stages):
+        ptrs[s] = a.ctypes.data_as(O._U64P)
+        lens[s] = len(a)
+    t0 = time.perf_counter()
+    st = lib.zo_ntt_with_twiddles_inplace4(O.BN254_FR, O._p(data), len(data), log_n, ptrs, lens, len(stages), 0,
+                                           workers)
+    dt = time.perf_counter() - t0
+    assert st == 0
+    return dt
+
+
+def cpu_reference_setup(log_n, seed, host_data=None):
+    O, lib = cpu_oracle(native=True)
+    n = 1 << log_n
+    data = host_data.copy() if host_data is not None else O.random_elements(O.BN254_FR, seed, n)
+    st, root = O.primitive_root(O.BN254_FR, log_n)
+    st, stages = O.precompute_twiddles(O.BN254_FR, log_n, root)
+    return O, lib, data, stages
+
+
+def run_reference(args, rank):
+    """The reference arm: zig-ntt's algorithm on the host cores (oracle port)."""
+    if rank != 0:
+        return
+    workers = min(os.cpu_count() or 1, 64)
+    log_n = args.log_n
+    n = 1 << log_n
+    O, lib, data, stages = cpu_reference_setup(log_n, args.seed)
+    for _ in range(args.warmup):
+        cpu_transform_seconds(O, lib, data, log_n, stages, workers)
+    times = [cpu_transform_seconds(O, lib, data, log_n, stages, workers) for _ in range(args.steps)]
+    total = sum(times)
+    value = n * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u256-mod-r (BN254-Fr)",
+        "data": "synthetic: seeded ChaCha20 randomFieldElement draws",
+        "config": {"workload": f"bn254_fr_ntt_forward_2^{log_n}", "log_n": log_n, "field": "bn254_fr",
+                   "direction": "forward", "twiddles": "precomputed", "threads": workers},
+        "cpu_baseline": {"value": value, "unit": "elements/s", "cores": workers, "kind": "port",
+                         "sample": f"{args.steps} full 2^{log_n} transforms, oracle nttWithTwiddles, "
+                                   f"fork-join over butterflies per stage"},
+        "e2e": {"value": value, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --- the GPU arm -------------------------------------------------------------------------
+
+def run_zntt(args, rank, world, local):
+    import torch
+    z = load_package()
+    torch.cuda.set_device(local)
+    z.init(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        pg = dist
+    F = z.BN254_FR
+    log_n = args.log_n
+    n = 1 << log_n
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    x = torch.empty(n * 4, dtype=torch.int64, device="cuda")
+    y = torch.empty_like(x)
+    z.random_elements(F, args.seed + rank, x.data_ptr(), n, stream=sptr)
+    root = z.primitiveRootOfUnity(F, log_n)
+    tw = z.DeviceTwiddles(F, log_n, root)
+    passes = len(__import__("math").ceil(log_n / 10) * [0]) if log_n > 11 else 1
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    # Warm-up, then exactly K timed steps bracketed by barrier + synchronize.
+    for _ in range(args.warmup):
+        z.ntt_device(tw, x.data_ptr(), y.data_ptr(), z.FORWARD, stream=sptr)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        z.ntt_device(tw, x.data_ptr(), y.data_ptr(), z.FORWARD, stream=sptr)
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if pg:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_step = ms_max / args.steps
+    value = world * n * args.steps / (ms_max * 1e-3)
+
+    # e2e through the host-buffer C ABI: pinned host input, H2D + transform + D2H per step.
+    hin = torch.empty(n * 4, dtype=torch.int64, pin_memory=True)
+    hin.copy_(x.cpu())
+    host = hin.numpy().view("uint64").reshape(n, 4)
+    orig = host.copy()
+    htw = z.precomputeTwiddles(F, log_n, root)
+    for _ in range(max(1, min(args.warmup, 2))):
+        host[:] = orig
+        z.nttWithTwiddles(F, host, log_n, htw)
+    e2e_steps = max(2, min(args.steps, 5))
+    barrier()
+    dts = []
+    for _ in range(e2e_steps):
+        host[:] = orig  # a fresh input each step (untimed host copy)
+        t0 = time.perf_counter()
+        z.nttWithTwiddles(F, host, log_n, htw)
+        dts.append(time.perf_counter() - t0)
+    e2e_s = torch.tensor([sum(dts)], dtype=torch.float64, device="cuda")
+    if pg:
+        pg.all_reduce(e2e_s, op=pg.ReduceOp.MAX)
+    e2e_value = world * n * e2e_steps / float(e2e_s.item())
+    # the e2e result must equal the device-resident result
+    ok = bool((torch.from_numpy(host.view("int64").reshape(-1)).cuda() == y).all().item())
+    z.freeTwiddles(F, htw)
+
+    # Roofline: the pass kernel is the only kernel in the timed region.
+    imad = z.probe_imad()
+    peak_modmul = imad / IMAD_PER_MODMUL
+    modmuls = n / 2 * log_n
+    achieved = modmuls / (ms_step * 1e-3)
+    peaks, peaks_kind = measured_peaks()
+    alg_bytes = 2 * n * 32
+    passes = __import__("math").ceil(log_n / 10) if log_n > 11 else 1
+    traffic = read_traffic(log_n)
+    tw.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u256-mod-r (BN254-Fr, 8x32-bit Montgomery)",
+        "data": "synthetic: seeded ChaCha20 randomFieldElement draws generated on the device",
+        "config": {"workload": f"bn254_fr_ntt_forward_2^{log_n}", "log_n": log_n, "field": "bn254_fr",
+                   "direction": "forward", "twiddles": "precomputed, device-resident",
+                   "l2": "inputs (512 MiB per vector) larger than L2; no flush", "passes": passes,
+                   "parallelism": f"replicas x{world} (independent vectors, no collective)"},
+        "e2e": {"value": e2e_value, "unit": "elements/s", "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 32,
+                "api": "zntt_ntt_with_twiddles (host buffers, pinned)", "matches_device_result": ok},
+        "gpu_launches": args.steps * passes,
+        "roofline": {"bound": "imad", "achieved": achieved, "peak": peak_modmul, "unit": "modmul/s",
+                     "frac": achieved / peak_modmul, "traffic": traffic,
+                     "peak_source": f"measured live: multiply-pipe probe {imad:.4g} mad/s / "
+                                    f"{IMAD_PER_MODMUL} per 8x32 CIOS product",
+                     "hbm": {"achieved": alg_bytes / (ms_step * 1e-3) / 1e9, "peak": peaks["hbm_gbs"],
+                             "unit": "GB/s", "frac": alg_bytes / (ms_step * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                             "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peaks_kind})"}},
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline_sample(orig, log_n)
+        except Exception as e:  # noqa: BLE001 -- report, never fail the GPU line
+            line["cpu_baseline"] = {"value": None, "error": str(e)}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(host_data, log_n):
+    """The oracle port on all host cores, on the same input, for one full transform."""
+    workers = min(os.cpu_count() or 1, 64)
+    O, lib, data, stages = cpu_reference_setup(log_n, 0, host_data)
+    dt = cpu_transform_seconds(O, lib, data, log_n, stages, workers)
+    reps = [dt]
+    while sum(reps) < 10.0 and len(reps) < 5:
+        data[:] = host_data
+        reps.append(cpu_transform_seconds(O, lib, data, log_n, stages, workers))
+    best = min(reps)
+    return {"value": (1 << log_n) / best, "unit": "elements/s", "cores": workers, "kind": "port",
+            "sample": f"{len(reps)} full 2^{log_n} forward transforms (best), oracle nttWithTwiddles, "
+                      f"fork-join over butterflies per stage"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="zntt", choices=["zntt", "reference"])
+    ap.add_argument("--log-n", type=int, default=24)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank)
+    else:
+        run_zntt(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,146 @@
+/* zntt.h -- C ABI of libzntt_cuda.so, the B200 (sm_100a) NTT library.
+ *
+ * The library replaces zig-algebra's NTT hot path, the Zig module `zig-ntt`
+ * (libs/ntt/src/root.zig), for the two scalar fields it runs on in practice:
+ * BN254-Fr (libs/curve/src/bn254.zig:67) and BLS12-381-Fr
+ * (libs/curve/src/bls12_381.zig:66).  An element is the reference's
+ * `BigField` value (libs/field/src/field.zig:884): four little-endian u64 limbs
+ * in Montgomery form (x * 2^256 mod r), fully reduced.  Every function takes
+ * plain pointers and sizes; arrays of elements are `4 * len` u64 words.
+ *
+ * Errors are integer status codes that map one to one onto zig-ntt's error
+ * set (libs/ntt/src/root.zig:33-36, 43, 67-68, 150-152, 161) plus the device
+ * failures a GPU adds.  Unlike zig-ntt, every argument is validated before
+ * any data moves: on any error `data` is left untouched (zig-ntt leaves a
+ * partially transformed buffer when a later twiddle stage has the wrong
+ * length, libs/ntt/src/root.zig:161).
+ *
+ * Thread safety: calls may come from any thread; the library serialises them
+ * on its own stream per device.  The plain entry points are synchronous, like
+ * the reference.
+ */
+#ifndef ZNTT_H
+#define ZNTT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum zntt_status {
+  ZNTT_OK = 0,
+  ZNTT_ERR_LOG_TOO_LARGE = 1,      /* error.LogTooLarge: log_n >= 64 (root.zig:33-36) */
+  ZNTT_ERR_LENGTH_MISMATCH = 2,    /* error.LengthMismatch: len != 2^log_n (root.zig:68) */
+  ZNTT_ERR_INVALID_TWIDDLES = 3,   /* error.InvalidTwiddles (root.zig:152, 161) */
+  ZNTT_ERR_INVALID_LENGTH = 4,     /* error.InvalidLength: bitReverse len 0 / not 2^k (root.zig:43) */
+  ZNTT_ERR_OUT_OF_MEMORY = 5,      /* error.OutOfMemory, or the vector does not fit on the device */
+  ZNTT_ERR_ORDER_TOO_LARGE = 6,    /* error.OrderTooLarge: log_n > two-adicity (roots.zig:150) */
+  ZNTT_ERR_UNSUPPORTED_FIELD = 7,  /* a field id other than the two below */
+  ZNTT_ERR_DEVICE = 8,             /* a CUDA call failed; see zntt_last_error() */
+  ZNTT_ERR_TIMEOUT = 9,            /* a bounded device wait gave up */
+  ZNTT_ERR_INVALID_ARGUMENT = 10,  /* null pointer, bad handle, unknown mode */
+  ZNTT_ERR_NOT_INITIALIZED = 11,   /* zntt_init() has not run */
+  ZNTT_ERR_REJECTED = 12           /* admission refused (over the memory budget / queue full) */
+};
+
+/* ---- fields ---------------------------------------------------------------- */
+enum zntt_field {
+  ZNTT_FIELD_BN254_FR = 0,      /* r = 0x30644e72...43e1f593f0000001, two-adicity 28 */
+  ZNTT_FIELD_BLS12_381_FR = 1   /* r = 0x73eda753...ffffffff00000001, two-adicity 32 */
+};
+
+/* One twiddle stage as zig-ntt hands it over: the layout of a Zig
+ * `[]const F` slice (pointer, element count). */
+typedef struct zntt_stage {
+  const uint64_t* ptr;
+  size_t len;
+} zntt_stage;
+
+/* ---- lifetime ------------------------------------------------------------- */
+/* Selects the CUDA device and creates the library's stream and caches.
+ * Idempotent for the same device. */
+int zntt_init(int device);
+/* Frees every device buffer, cache entry and stream. */
+int zntt_shutdown(void);
+/* Message of the last failure on the calling thread ("" when none). */
+const char* zntt_last_error(void);
+/* Modulus (canonical, 4 LE limbs) and two-adicity of a field. */
+int zntt_field_info(int field, uint64_t modulus[4], uint32_t* two_adicity);
+/* F.primitiveRootOfUnity(log_n) in Montgomery form: the first quadratic
+ * non-residue counting up from 2 (5 for both fields) raised to
+ * odd_part << (two_adicity - log_n) (libs/field/src/roots.zig:149-158). */
+int zntt_primitive_root(int field, uint32_t log_n, uint64_t root_out[4]);
+
+/* ---- zig-ntt drop-in: host data, synchronous -------------------------------
+ * Each replaces the zig-ntt function named in its comment; `field` stands in
+ * for the `comptime F` parameter. */
+
+/* bitReverse(F, data)            libs/ntt/src/root.zig:38-58 */
+int zntt_bit_reverse(uint64_t* data, size_t len);
+/* ntt(F, data, log_n, root)       libs/ntt/src/root.zig:65-90 */
+int zntt_ntt(int field, uint64_t* data, size_t len, size_t log_n, const uint64_t root[4]);
+/* intt(F, data, log_n, root)      libs/ntt/src/root.zig:95-107 */
+int zntt_intt(int field, uint64_t* data, size_t len, size_t log_n, const uint64_t root[4]);
+/* precomputeTwiddles(F, log_n, root, allocator)   libs/ntt/src/root.zig:112-134
+ * The caller allocates the table as zig-ntt's allocator would (stage s:
+ * 2^s elements) and passes the stage pointers; the library fills them from
+ * the device and keeps the same table resident on the device, recognised
+ * again by its stage addresses. */
+int zntt_precompute_twiddles(int field, size_t log_n, const uint64_t root[4], uint64_t* const* stage_out);
+/* freeTwiddles(F, twiddles, allocator)            libs/ntt/src/root.zig:136-141
+ * Releases the device copy; the caller frees its own stage arrays. */
+void zntt_free_twiddles(int field, const zntt_stage* stages, size_t num_stages);
+/* nttWithTwiddles(F, data, log_n, twiddles)       libs/ntt/src/root.zig:148-175 */
+int zntt_ntt_with_twiddles(int field, uint64_t* data, size_t len, size_t log_n, const zntt_stage* stages,
+                           size_t num_stages);
+/* inttWithTwiddles(F, data, log_n, twiddles)      libs/ntt/src/root.zig:180-212 */
+int zntt_intt_with_twiddles(int field, uint64_t* data, size_t len, size_t log_n, const zntt_stage* stages,
+                            size_t num_stages);
+
+/* ---- device-resident API ------------------------------------------------------
+ * For callers that keep vectors in HBM.  `stream` is a cudaStream_t (NULL: the
+ * library's stream); calls are asynchronous on it. */
+typedef struct zntt_twiddles zntt_twiddles;
+
+/* Device twiddle table for (field, log_n, root), shared and reference counted:
+ * the table precomputeTwiddles would build, kept on the device. */
+int zntt_twiddles_acquire(int field, uint32_t log_n, const uint64_t root[4], zntt_twiddles** out);
+int zntt_twiddles_release(zntt_twiddles* tw);
+
+enum zntt_mode {
+  ZNTT_FORWARD = 0,  /* nttWithTwiddles */
+  ZNTT_INVERSE = 1   /* inttWithTwiddles (includes the 1/n scale) */
+};
+
+/* Transform 2^log_n device elements from d_src into d_dst (which may equal
+ * d_src).  `d_scratch` (2^log_n elements, or NULL) is only used when
+ * d_dst == d_src and the transform needs more than one pass; when NULL the
+ * library borrows one from its pool. */
+int zntt_ntt_device(const zntt_twiddles* tw, const uint64_t* d_src, uint64_t* d_dst, uint64_t* d_scratch,
+                    int mode, void* stream);
+
+/* Seeded uniform elements on the device: element i is the i-th
+ * randomFieldElement draw (libs/rng/src/rng.zig:32-65) from the ChaCha20
+ * stream keyed by seed32 with a zero nonce and counter from 0
+ * (libs/rng/src/chacha20.zig:81-110), in Montgomery form. */
+int zntt_random_elements(int field, const uint8_t seed32[32], uint64_t* d_out, size_t count, void* stream);
+
+/* Elementwise device arithmetic (op 0 mul, 1 add, 2 sub, 3 neg) over `count`
+ * device elements; exposed for the arithmetic parity tests. */
+int zntt_elementwise_device(int field, int op, const uint64_t* d_a, const uint64_t* d_b, uint64_t* d_out,
+                            size_t count, void* stream);
+
+/* ---- roofline probes ---------------------------------------------------------
+ * Throughput of the multiply pipe and of the field product on this device,
+ * measured with CUDA events; used as the roofline denominator. */
+int zntt_probe_imad(double* imad_per_second);
+int zntt_probe_modmul(int field, double* modmul_per_second);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZNTT_H */

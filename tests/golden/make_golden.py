@@ -1,0 +1,143 @@
+"""Regenerates the golden fixtures in this folder.
+
+    python tests/golden/make_golden.py [--reference PATH]
+
+Two kinds of fixture:
+
+1. Vectors copied as data from the reference's own tests, read as text:
+   * ntt_kat.json -- the known-answer DFT cases of libs/ntt/src/root.zig:438-449
+     (Goldilocks and BabyBear, log_n 1-4, root / input / expected output).
+   * chacha20_rfc8439.json -- the RFC 8439 keystream vectors that
+     libs/rng/src/root.zig:182-228 checks the reference's ChaCha20 against.
+2. Vectors computed here by pyref.py (pure Python, independent of the oracle
+   and of the CUDA library) for the two scalar fields the transform serves:
+   * fr_transforms.json -- seeded randomFieldElement inputs (ChaCha20, seed
+     encoding u64 LE + zeros), the reference-derived primitive roots, and the
+     forward / inverse transforms by definition (n <= 2^6) or by a radix-2 FFT
+     checked against the definition (n = 2^12, the plain 2^12 BN254-Fr case).
+   * coset_lde.json -- a small blowup-4 coset extension over BLS12-381-Fr with
+     shift 5, the reference's quadratic non-residue.
+
+Values are canonical (not Montgomery) hex strings.  Large vectors are stored as
+a SHA-256 of their little-endian 32-byte encoding plus a few leading values.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import re
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import pyref  # noqa: E402
+
+
+def vec_digest(values: list[int]) -> str:
+    h = hashlib.sha256()
+    for v in values:
+        h.update(int(v).to_bytes(32, "little"))
+    return h.hexdigest()
+
+
+def parse_kats(ref: str) -> list[dict]:
+    path = os.path.join(ref, "libs/ntt/src/root.zig")
+    lines = open(path).read().splitlines()
+    cases = []
+    field = None
+    for ln, text in enumerate(lines, start=1):
+        if text.strip() == "// Goldilocks":
+            field = "goldilocks"
+        elif text.strip() == "// BabyBear":
+            field = "babybear"
+        m = re.search(r"\.log_n = (\d+), \.root = (0x[0-9a-f]+), \.input = &\.\{ ([^}]*) \}, "
+                      r"\.expect = &\.\{ ([^}]*) \}", text)
+        if m and field:
+            cases.append({
+                "field": field,
+                "log_n": int(m.group(1)),
+                "root": m.group(2),
+                "input": [s.strip() for s in m.group(3).split(",")],
+                "expect": [s.strip() for s in m.group(4).split(",")],
+                "source": f"libs/ntt/src/root.zig:{ln}",
+            })
+    assert len(cases) == 8, len(cases)
+    return cases
+
+
+def parse_rfc(ref: str) -> dict:
+    path = os.path.join(ref, "libs/rng/src/root.zig")
+    text = open(path).read()
+    hexes = re.findall(r'hexToBytes\(&want_\w+, "([0-9a-f]+)"\)', text)
+    plain = re.search(r'const plaintext = "([^"]+)";', text).group(1)
+    assert len(hexes) == 3
+    return {
+        "key": bytes(range(32)).hex(),
+        "block_nonce": "000000090000004a00000000",
+        "block_counter1": hexes[0],
+        "cipher_nonce": "000000000000004a00000000",
+        "keystream_counter1": hexes[1],
+        "ciphertext": hexes[2],
+        "plaintext": plain,
+        "source": "libs/rng/src/root.zig:182-228 (RFC 8439 sections 2.3.2 and 2.4.2)",
+    }
+
+
+def fr_cases() -> list[dict]:
+    out = []
+    plan = [("bn254_fr", pyref.BN254_FR_P, [1, 2, 3, 4, 5, 6], 101),
+            ("bls12_381_fr", pyref.BLS12_381_FR_P, [1, 2, 3, 4, 5, 6], 202)]
+    for name, p, logs, seed0 in plan:
+        for log_n in logs:
+            n = 1 << log_n
+            seed = seed0 + log_n
+            x = pyref.random_field_values(p, seed, n)
+            w = pyref.primitive_root(p, log_n)
+            fwd = pyref.dft(x, w, p)
+            assert pyref.fft(x, w, p) == fwd
+            inv = pyref.inverse_transform(x, w, p)
+            out.append({"field": name, "log_n": log_n, "seed": seed, "root": hex(w),
+                        "input": [hex(v) for v in x], "forward": [hex(v) for v in fwd],
+                        "inverse": [hex(v) for v in inv]})
+    # The plain 2^12 BN254-Fr transform: forward by FFT, inverse round trip.
+    p, log_n, seed = pyref.BN254_FR_P, 12, 12
+    x = pyref.random_field_values(p, seed, 1 << log_n)
+    w = pyref.primitive_root(p, log_n)
+    fwd = pyref.fft(x, w, p)
+    inv = pyref.inverse_transform(x, w, p)
+    # Spot-check the FFT against the definition at a few indices.
+    for k in (0, 1, 7, 2048, 4095):
+        assert fwd[k] == sum(x[j] * pow(w, j * k, p) for j in range(len(x))) % p
+    out.append({"field": "bn254_fr", "log_n": log_n, "seed": seed, "root": hex(w),
+                "input_sha256": vec_digest(x), "input_head": [hex(v) for v in x[:8]],
+                "forward_sha256": vec_digest(fwd), "forward_head": [hex(v) for v in fwd[:8]],
+                "inverse_sha256": vec_digest(inv), "inverse_head": [hex(v) for v in inv[:8]]})
+    return out
+
+
+def lde_case() -> dict:
+    p = pyref.BLS12_381_FR_P
+    log_in, log_blowup, seed = 6, 2, 303
+    evals = pyref.random_field_values(p, seed, 1 << log_in)
+    shift = pyref.first_qnr(p)
+    assert shift == 5
+    out = pyref.coset_lde(evals, log_blowup, shift, p)
+    return {"field": "bls12_381_fr", "log_in": log_in, "log_blowup": log_blowup, "seed": seed,
+            "shift": shift, "evals": [hex(v) for v in evals], "output": [hex(v) for v in out]}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    args = ap.parse_args()
+    json.dump(parse_kats(args.reference), open(os.path.join(HERE, "ntt_kat.json"), "w"), indent=1)
+    json.dump(parse_rfc(args.reference), open(os.path.join(HERE, "chacha20_rfc8439.json"), "w"), indent=1)
+    json.dump(fr_cases(), open(os.path.join(HERE, "fr_transforms.json"), "w"), indent=1)
+    json.dump(lde_case(), open(os.path.join(HERE, "coset_lde.json"), "w"), indent=1)
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

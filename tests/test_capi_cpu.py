@@ -1,0 +1,92 @@
+"""C-ABI checks that need no GPU: the library loads, exports every declared
+entry point, validates arguments in zig-ntt's error order before touching a
+device (libs/ntt/src/root.zig:33-36, 43, 67-68, 150-152, 161), and computes
+the host-side set-up values (roots of unity) exactly like the reference."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+
+def test_library_exports_every_declared_symbol(zntt):
+    declared = zntt.declared_symbols()
+    assert len(declared) >= 19
+    L = zntt.lib()
+    missing = [s for s in declared if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_field_info(zntt):
+    for F in zntt.FIELDS:
+        mod = (ctypes.c_uint64 * 4)()
+        adic = ctypes.c_uint32()
+        assert zntt.lib().zntt_field_info(F.id, mod, ctypes.byref(adic)) == 0
+        assert sum(int(v) << (64 * k) for k, v in enumerate(mod)) == F.modulus
+        assert adic.value == F.two_adicity
+    with pytest.raises(zntt.UnsupportedField):
+        zntt._check(zntt.lib().zntt_field_info(7, mod, ctypes.byref(adic)))
+
+
+@pytest.mark.parametrize("fname", ["bn254_fr", "bls12_381_fr"])
+def test_primitive_root_matches_reference_derivation(zntt, oracle, fname):
+    F = getattr(zntt, fname.upper())
+    fid = {"bn254_fr": O.BN254_FR, "bls12_381_fr": O.BLS12_381_FR}[fname]
+    for log_n in [0, 1, 2, 5, 12, 20, 24, F.two_adicity]:
+        st, want = O.primitive_root(fid, log_n)
+        assert st == 0
+        got = zntt.primitiveRootOfUnity(F, log_n)
+        np.testing.assert_array_equal(got, want)
+    with pytest.raises(zntt.OrderTooLarge):
+        zntt.primitiveRootOfUnity(F, F.two_adicity + 1)
+
+
+def test_shape_errors_are_reported_before_any_device_work(zntt):
+    F = zntt.BN254_FR
+    root = zntt.primitiveRootOfUnity(F, 2)
+    short = np.zeros((3, 4), dtype=np.uint64)
+    with pytest.raises(zntt.LengthMismatch):
+        zntt.ntt(F, short, 2, root)
+    with pytest.raises(zntt.LengthMismatch):
+        zntt.intt(F, short, 2, root)
+    two = np.zeros((2, 4), dtype=np.uint64)
+    with pytest.raises(zntt.LogTooLarge):
+        zntt.ntt(F, two, 64, root)
+    with pytest.raises(zntt.LogTooLarge):
+        zntt.intt(F, two, 200, root)
+    with pytest.raises(zntt.LogTooLarge):
+        zntt.precomputeTwiddles(F, 64, root)
+    with pytest.raises(zntt.InvalidLength):
+        zntt.bitReverse(F, np.zeros((0, 4), dtype=np.uint64))
+    with pytest.raises(zntt.InvalidLength):
+        zntt.bitReverse(F, np.zeros((3, 4), dtype=np.uint64))
+    data = np.zeros((8, 4), dtype=np.uint64)
+    fake = [np.zeros((1 << s, 4), dtype=np.uint64) for s in range(3)]
+    # table shorter than log_n
+    with pytest.raises(zntt.InvalidTwiddles):
+        zntt.nttWithTwiddles(F, data, 3, fake[:2])
+    with pytest.raises(zntt.InvalidTwiddles):
+        zntt.inttWithTwiddles(F, data, 3, fake[:2])
+    # a stage of the wrong length
+    with pytest.raises(zntt.InvalidTwiddles):
+        zntt.nttWithTwiddles(F, data, 3, [fake[0], fake[1][:1], fake[2]])
+    # order: LogTooLarge, then LengthMismatch, then InvalidTwiddles
+    with pytest.raises(zntt.LogTooLarge):
+        zntt.nttWithTwiddles(F, np.zeros((3, 4), dtype=np.uint64), 64, [])
+    with pytest.raises(zntt.LengthMismatch):
+        zntt.nttWithTwiddles(F, np.zeros((3, 4), dtype=np.uint64), 3, [])
+    # on every error the data is untouched (validation precedes any mutation)
+    d = np.arange(32, dtype=np.uint64).reshape(8, 4).copy()
+    before = d.copy()
+    with pytest.raises(zntt.InvalidTwiddles):
+        zntt.nttWithTwiddles(F, d, 3, [fake[0], fake[1][:1], fake[2]])
+    np.testing.assert_array_equal(d, before)
+
+
+def test_unsupported_field_rejected(zntt):
+    bogus = zntt.Field(9, "bogus", 7, 1)
+    with pytest.raises(zntt.UnsupportedField):
+        zntt.ntt(bogus, np.zeros((2, 4), dtype=np.uint64), 1, np.zeros(4, dtype=np.uint64))

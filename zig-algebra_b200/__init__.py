@@ -1,0 +1,357 @@
+"""Host-side mirror of zig-ntt over the B200 library libzntt_cuda.so.
+
+zig-ntt (libs/ntt/src/root.zig) is a Zig module whose functions take the field
+type as a `comptime F` argument; here the field is a `Field` object and the
+data is a numpy uint64 array of shape (n, 4) holding the reference's [4]u64
+Montgomery limbs per element (C-contiguous, transformed in place).  Names,
+argument meaning and error behaviour follow zig-ntt:
+
+    bitReverse(F, data)                       root.zig:38-58
+    ntt(F, data, log_n, root)                 root.zig:65-90
+    intt(F, data, log_n, root)                root.zig:95-107
+    precomputeTwiddles(F, log_n, root)        root.zig:112-134
+    freeTwiddles(F, twiddles)                 root.zig:136-141
+    nttWithTwiddles(F, data, log_n, tw)       root.zig:148-175
+    inttWithTwiddles(F, data, log_n, tw)      root.zig:180-212
+
+Each zig-ntt error is an exception class of the same name.  Every transform
+runs on the GPU; if the CUDA library or a device is missing the calls raise,
+there is no CPU fallback.  The device-resident API (`DeviceTwiddles`,
+`ntt_device`, `random_elements`) works on raw device pointers, e.g. from
+`torch.Tensor.data_ptr()`.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libzntt_cuda.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "zntt.h")
+
+
+# --- errors (zig-ntt's error set plus device failures) ------------------------
+
+class ZnttError(Exception):
+    code = -1
+
+
+class LogTooLarge(ZnttError):
+    code = 1
+
+
+class LengthMismatch(ZnttError):
+    code = 2
+
+
+class InvalidTwiddles(ZnttError):
+    code = 3
+
+
+class InvalidLength(ZnttError):
+    code = 4
+
+
+class OutOfMemory(ZnttError):
+    code = 5
+
+
+class OrderTooLarge(ZnttError):
+    code = 6
+
+
+class UnsupportedField(ZnttError):
+    code = 7
+
+
+class DeviceError(ZnttError):
+    code = 8
+
+
+class Timeout(ZnttError):
+    code = 9
+
+
+class InvalidArgument(ZnttError):
+    code = 10
+
+
+class NotInitialized(ZnttError):
+    code = 11
+
+
+class Rejected(ZnttError):
+    code = 12
+
+
+_ERRORS = {c.code: c for c in (LogTooLarge, LengthMismatch, InvalidTwiddles, InvalidLength, OutOfMemory,
+                               OrderTooLarge, UnsupportedField, DeviceError, Timeout, InvalidArgument,
+                               NotInitialized, Rejected)}
+
+
+# --- fields ----------------------------------------------------------------------
+
+class Field:
+    """A scalar field served by the library (the `comptime F` of zig-ntt)."""
+
+    def __init__(self, fid: int, name: str, modulus: int, two_adicity: int):
+        self.id, self.name, self.modulus, self.two_adicity = fid, name, modulus, two_adicity
+
+    def __repr__(self):
+        return f"Field({self.name})"
+
+
+BN254_FR = Field(0, "bn254_fr", 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001, 28)
+BLS12_381_FR = Field(1, "bls12_381_fr", 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001, 32)
+FIELDS = (BN254_FR, BLS12_381_FR)
+
+FORWARD = 0
+INVERSE = 1
+
+
+# --- library loading ------------------------------------------------------------------
+
+class _Stage(ctypes.Structure):
+    _fields_ = [("ptr", ctypes.POINTER(ctypes.c_uint64)), ("len", ctypes.c_size_t)]
+
+
+_U64P = ctypes.POINTER(ctypes.c_uint64)
+_lib = None
+_device = None
+
+
+def lib():
+    """The loaded CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run zig-algebra_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        sz, i, vp = ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p
+        L.zntt_init.argtypes = [i]
+        L.zntt_last_error.restype = ctypes.c_char_p
+        L.zntt_field_info.argtypes = [i, _U64P, ctypes.POINTER(ctypes.c_uint32)]
+        L.zntt_primitive_root.argtypes = [i, ctypes.c_uint32, _U64P]
+        L.zntt_bit_reverse.argtypes = [_U64P, sz]
+        L.zntt_ntt.argtypes = [i, _U64P, sz, sz, _U64P]
+        L.zntt_intt.argtypes = [i, _U64P, sz, sz, _U64P]
+        L.zntt_precompute_twiddles.argtypes = [i, sz, _U64P, ctypes.POINTER(_U64P)]
+        L.zntt_free_twiddles.argtypes = [i, ctypes.POINTER(_Stage), sz]
+        L.zntt_free_twiddles.restype = None
+        L.zntt_ntt_with_twiddles.argtypes = [i, _U64P, sz, sz, ctypes.POINTER(_Stage), sz]
+        L.zntt_intt_with_twiddles.argtypes = [i, _U64P, sz, sz, ctypes.POINTER(_Stage), sz]
+        L.zntt_twiddles_acquire.argtypes = [i, ctypes.c_uint32, _U64P, ctypes.POINTER(vp)]
+        L.zntt_twiddles_release.argtypes = [vp]
+        L.zntt_ntt_device.argtypes = [vp, vp, vp, vp, i, vp]
+        L.zntt_random_elements.argtypes = [i, ctypes.c_char_p, vp, sz, vp]
+        L.zntt_elementwise_device.argtypes = [i, i, vp, vp, vp, sz, vp]
+        L.zntt_probe_imad.argtypes = [ctypes.POINTER(ctypes.c_double)]
+        L.zntt_probe_modmul.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
+        _lib = L
+    return _lib
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        msg = lib().zntt_last_error().decode(errors="replace")
+        if status == NotInitialized.code and _init_failure is not None:
+            msg = f"{msg}; device initialisation failed: {_init_failure}"
+        raise _ERRORS.get(status, ZnttError)(msg or f"status {status}")
+
+
+def init(device: int = 0) -> None:
+    """Binds the library to a CUDA device (idempotent)."""
+    global _device, _init_failure
+    _check(lib().zntt_init(device))
+    _device = device
+    _init_failure = None
+
+
+_init_failure = None
+
+
+def _ensure_init() -> None:
+    """Binds the default device once.  A failure is remembered, not raised, so
+    argument errors still surface first (the library validates before it
+    touches the device) and a device-needing call then raises NotInitialized."""
+    global _init_failure
+    if _device is None and _init_failure is None:
+        try:
+            init(int(os.environ.get("LOCAL_RANK", "0")))
+        except ZnttError as e:
+            _init_failure = e
+
+
+def shutdown() -> None:
+    global _device
+    lib().zntt_shutdown()
+    _device = None
+
+
+def declared_symbols() -> list[str]:
+    """Entry points declared in include/zntt.h."""
+    import re
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:const char\*|int|void)\s+(zntt_\w+)\(", text, re.M)))
+
+
+# --- element helpers ---------------------------------------------------------------
+
+def _p(a: np.ndarray):
+    if a.dtype != np.uint64 or not a.flags["C_CONTIGUOUS"] or a.ndim != 2 or a.shape[1] != 4:
+        raise InvalidArgument("data must be a C-contiguous uint64 array of shape (n, 4)")
+    return a.ctypes.data_as(_U64P)
+
+
+def _root(root) -> ctypes.Array:
+    r = np.ascontiguousarray(np.asarray(root, dtype=np.uint64).reshape(4))
+    return (ctypes.c_uint64 * 4)(*[int(v) for v in r])
+
+
+def primitiveRootOfUnity(F: Field, log_n: int) -> np.ndarray:
+    """F.primitiveRootOfUnity(log_n) (libs/field/src/roots.zig:149-158), Montgomery limbs."""
+    out = (ctypes.c_uint64 * 4)()
+    _check(lib().zntt_primitive_root(F.id, log_n, out))
+    return np.array(list(out), dtype=np.uint64)
+
+
+# --- zig-ntt mirror --------------------------------------------------------------------
+
+def bitReverse(F: Field, data: np.ndarray) -> None:
+    _ensure_init()
+    _check(lib().zntt_bit_reverse(_p(data), len(data)))
+
+
+def ntt(F: Field, data: np.ndarray, log_n: int, root) -> None:
+    _ensure_init()
+    _check(lib().zntt_ntt(F.id, _p(data), len(data), log_n, _root(root)))
+
+
+def intt(F: Field, data: np.ndarray, log_n: int, root) -> None:
+    _ensure_init()
+    _check(lib().zntt_intt(F.id, _p(data), len(data), log_n, _root(root)))
+
+
+class Twiddles(list):
+    """zig-ntt's `[]const []const F`: stage s is an (2^s, 4) uint64 array."""
+
+    def __init__(self, F: Field, stages):
+        super().__init__(stages)
+        self.field = F
+        self.registered = False
+
+    def stage_array(self):
+        arr = (_Stage * max(len(self), 1))()
+        for s, a in enumerate(self):
+            if a.dtype != np.uint64 or not a.flags["C_CONTIGUOUS"]:
+                raise InvalidTwiddles("stage arrays must be C-contiguous uint64")
+            arr[s].ptr = a.ctypes.data_as(_U64P)
+            arr[s].len = len(a)
+        return arr
+
+
+def precomputeTwiddles(F: Field, log_n: int, root) -> Twiddles:
+    if log_n >= 64:
+        _check(1)
+    stages = [np.zeros((1 << s, 4), dtype=np.uint64) for s in range(log_n)]
+    ptrs = (_U64P * max(log_n, 1))()
+    for s, a in enumerate(stages):
+        ptrs[s] = a.ctypes.data_as(_U64P)
+    _ensure_init()
+    _check(lib().zntt_precompute_twiddles(F.id, log_n, _root(root), ptrs))
+    tw = Twiddles(F, stages)
+    tw.registered = True
+    return tw
+
+
+def freeTwiddles(F: Field, twiddles: Twiddles) -> None:
+    if getattr(twiddles, "registered", False) and len(twiddles):
+        lib().zntt_free_twiddles(F.id, twiddles.stage_array(), len(twiddles))
+        twiddles.registered = False
+
+
+def _as_stages(F: Field, twiddles) -> Twiddles:
+    return twiddles if isinstance(twiddles, Twiddles) else Twiddles(F, list(twiddles))
+
+
+def nttWithTwiddles(F: Field, data: np.ndarray, log_n: int, twiddles) -> None:
+    tw = _as_stages(F, twiddles)
+    _ensure_init()
+    _check(lib().zntt_ntt_with_twiddles(F.id, _p(data), len(data), log_n, tw.stage_array(), len(tw)))
+
+
+def inttWithTwiddles(F: Field, data: np.ndarray, log_n: int, twiddles) -> None:
+    tw = _as_stages(F, twiddles)
+    _ensure_init()
+    _check(lib().zntt_intt_with_twiddles(F.id, _p(data), len(data), log_n, tw.stage_array(), len(tw)))
+
+
+# snake_case aliases
+bit_reverse = bitReverse
+precompute_twiddles = precomputeTwiddles
+free_twiddles = freeTwiddles
+ntt_with_twiddles = nttWithTwiddles
+intt_with_twiddles = inttWithTwiddles
+primitive_root_of_unity = primitiveRootOfUnity
+
+
+# --- device-resident API -------------------------------------------------------------------
+
+class DeviceTwiddles:
+    """A device twiddle table for (field, log_n, root), released on close()."""
+
+    def __init__(self, F: Field, log_n: int, root):
+        _ensure_init()
+        h = ctypes.c_void_p()
+        _check(lib().zntt_twiddles_acquire(F.id, log_n, _root(root), ctypes.byref(h)))
+        self.field, self.log_n, self.handle = F, log_n, h
+
+    def close(self) -> None:
+        if self.handle:
+            _check(lib().zntt_twiddles_release(self.handle))
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def ntt_device(tw: DeviceTwiddles, d_src: int, d_dst: int, mode: int = FORWARD, d_scratch: int = 0,
+               stream: int = 0) -> None:
+    """Transforms 2^tw.log_n device elements (pointers as ints) on `stream`."""
+    _check(lib().zntt_ntt_device(tw.handle, d_src, d_dst, d_scratch or None, mode, stream or None))
+
+
+def seed_bytes(seed: int) -> bytes:
+    """The 32-byte ChaCha20 key for an integer seed: u64 little-endian, then zeros."""
+    return int(seed).to_bytes(8, "little") + b"\x00" * 24
+
+
+def random_elements(F: Field, seed: int, d_out: int, count: int, stream: int = 0) -> None:
+    """Seeded randomFieldElement draws written to device memory (Montgomery form)."""
+    _ensure_init()
+    _check(lib().zntt_random_elements(F.id, seed_bytes(seed), d_out, count, stream or None))
+
+
+def elementwise_device(F: Field, op: str, d_a: int, d_b: int, d_out: int, count: int, stream: int = 0) -> None:
+    code = {"mul": 0, "add": 1, "sub": 2, "neg": 3}[op]
+    _ensure_init()
+    _check(lib().zntt_elementwise_device(F.id, code, d_a, d_b or None, d_out, count, stream or None))
+
+
+def probe_imad() -> float:
+    _ensure_init()
+    v = ctypes.c_double()
+    _check(lib().zntt_probe_imad(ctypes.byref(v)))
+    return v.value
+
+
+def probe_modmul(F: Field) -> float:
+    _ensure_init()
+    v = ctypes.c_double()
+    _check(lib().zntt_probe_modmul(F.id, ctypes.byref(v)))
+    return v.value

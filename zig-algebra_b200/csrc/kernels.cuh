@@ -1,0 +1,66 @@
+// kernels.cuh -- launch interface between the host runtime and the sm_100a kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace zntt {
+
+// Field identifiers shared with the C ABI (include/zntt.h).
+enum FieldId : int { kBn254Fr = 0, kBls12381Fr = 1 };
+
+// One fused radix-2^k pass of the decimation-in-time network.
+//
+// The network is zig-ntt's (libs/ntt/src/root.zig:148-212): bit-reverse the
+// input, then stages s = 1..log_n; stage s pairs positions q and q + 2^(s-1)
+// inside blocks of 2^s and uses twiddle tw[s-1][q mod 2^(s-1)].  A pass runs
+// stages S+1..S+k on tiles of 2^k positions that differ only in bits
+// [S, S+k) of q, with 2^c neighbouring low-bit positions per tile so global
+// rows are 2^c * 32 contiguous bytes.  The first pass (S == 0) gathers its
+// tile from the natural-order input, which folds the bit reversal into the
+// load: permuted block rev(col) holds input column col of the 2^k x 2^(L-k)
+// row-major view, row r landing at tile row rev_k(r).
+struct PassParams {
+  const uint4* src;   // 2 uint4 per element
+  uint4* dst;
+  const uint4* tw;    // zig-ntt twiddle table, stage s at entry 2^s - 1
+  uint32_t log_n;     // L
+  uint32_t S;         // stages already applied
+  uint32_t k;         // stages in this pass
+  uint32_t c;         // log2 of contiguous positions per tile row
+  uint32_t first;     // gather the input through the bit reversal
+  uint32_t inverse;   // inttWithTwiddles mapping: w = 1 (j = 0) or -tw[s-1][2^(s-1) - j]
+  uint32_t tw0_one;   // every stage's entry 0 is one (j = 0 needs no multiply)
+  uint32_t scale;     // multiply each output by scale_val after the last stage
+  uint32_t scale_val[8];
+};
+
+constexpr int kPassThreads = 256;
+constexpr int kLogTile = 11;                      // 2048 elements = 64 KiB of shared memory
+constexpr int kPassSmemBytes = (1 << kLogTile) * 32;
+
+cudaError_t launch_ntt_pass(int field, const PassParams& pp, uint64_t num_tiles, cudaStream_t st);
+cudaError_t configure_kernels();
+
+// Flat zig-ntt twiddle table for one (field, log_n, root): entry 2^s - 1 + j
+// of stage s is root^(j * 2^(log_n-1-s)).  The powers are assembled from three
+// small host-made tables: pw[0][i] = root^i, pw[1][i] = root^(1024 i),
+// pw[2][i] = root^(2^20 i), i < 1024 (each 1024 x 32 bytes, contiguous).
+cudaError_t launch_twiddle_table(int field, const uint4* d_pw, uint4* d_table, uint32_t log_n,
+                                 cudaStream_t st);
+
+// dst[rev(i)] = src[i] for 2^log_n elements (out of place).
+cudaError_t launch_bit_reverse(const uint4* src, uint4* dst, uint32_t log_n, cudaStream_t st);
+
+// Elementwise device arithmetic for tests: op 0 mul, 1 add, 2 sub, 3 neg.
+cudaError_t launch_elementwise(int field, int op, const uint4* a, const uint4* b, uint4* out,
+                               uint64_t count, cudaStream_t st);
+
+// Multiply-throughput probe: `iters` rounds of 8-long mad.lo/madc.hi carry
+// chains per thread; returns through `sink` so nothing is optimised away.
+cudaError_t launch_imad_probe(uint32_t* sink, uint32_t iters, int blocks, int threads, cudaStream_t st);
+// Independent modular products per thread, to time the field multiply alone.
+cudaError_t launch_modmul_probe(int field, uint4* sink, uint32_t iters, int blocks, int threads,
+                                cudaStream_t st);
+
+}  // namespace zntt

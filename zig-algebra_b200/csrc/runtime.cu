@@ -1,0 +1,814 @@
+// runtime.cu -- host runtime and the zig-ntt drop-in C ABI (include/zntt.h).
+//
+// The drop-in functions keep zig-ntt's argument meaning and error order
+// (libs/ntt/src/root.zig:33-212) and run every transform on the GPU: the
+// host vector is copied to HBM, transformed by the pass kernels in
+// kernels.cu, and copied back.  There is no CPU path: a missing or failing
+// device is an error, never a fallback.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "runtime.hpp"
+
+namespace zntt {
+
+// ---------------------------------------------------------------------------
+// errors and context
+// ---------------------------------------------------------------------------
+
+static thread_local std::string g_last_error;
+
+int set_error(int status, const std::string& msg) {
+  g_last_error = msg;
+  return status;
+}
+void clear_error() { g_last_error.clear(); }
+
+int cuda_fail(cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  if (e == cudaErrorMemoryAllocation) return set_error(ZNTT_ERR_OUT_OF_MEMORY, m);
+  return set_error(ZNTT_ERR_DEVICE, m);
+}
+
+Context& ctx() {
+  static Context c;
+  return c;
+}
+
+#define ZCHECK(call, what)                      \
+  do {                                          \
+    cudaError_t e_ = (call);                    \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// buffer pool
+// ---------------------------------------------------------------------------
+
+cudaError_t BufferPool::acquire(size_t bytes, void** out) {
+  auto it = free_.find(bytes);
+  if (it != free_.end()) {
+    *out = it->second;
+    free_.erase(it);
+    cached_ -= bytes;
+    return cudaSuccess;
+  }
+  cudaError_t e = cudaMalloc(out, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    trim();
+    e = cudaMalloc(out, bytes);
+  }
+  return e;
+}
+
+void BufferPool::release(void* p, size_t bytes) {
+  if (!p) return;
+  free_.emplace(bytes, p);
+  cached_ += bytes;
+}
+
+void BufferPool::trim() {
+  for (auto& kv : free_) cudaFree(kv.second);
+  free_.clear();
+  cached_ = 0;
+}
+
+// RAII pool buffer.
+struct PoolBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~PoolBuf() {
+    if (p) ctx().pool.release(p, bytes);
+  }
+  int get(size_t b) {
+    bytes = b;
+    cudaError_t e = ctx().pool.acquire(b, &p);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return cuda_fail(e, "device buffer");
+    }
+    return ZNTT_OK;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// pass planning
+// ---------------------------------------------------------------------------
+
+// Up to kLogTile stages run in one pass on a single tile of 2^log_n <= 2^kLogTile
+// elements.  Longer transforms are split into P = ceil(log_n / (kLogTile - 1))
+// passes of near-equal stage counts; each tile keeps 2^kLogTile elements, the
+// spare bits becoming 2^c contiguous positions per tile row.
+std::vector<PassDesc> plan_passes(uint32_t log_n) {
+  std::vector<PassDesc> out;
+  if (log_n == 0) return out;
+  if (log_n <= (uint32_t)kLogTile) {
+    out.push_back({0, log_n, 0});
+    return out;
+  }
+  const uint32_t kmax = kLogTile - 1;
+  const uint32_t P = (log_n + kmax - 1) / kmax;
+  uint32_t S = 0;
+  for (uint32_t p = 0; p < P; p++) {
+    uint32_t k = log_n / P + (p < log_n % P ? 1 : 0);
+    uint32_t c = kLogTile - k;
+    uint32_t lim = p == 0 ? log_n - k : S;  // columns available to a tile
+    if (c > lim) c = lim;
+    out.push_back({S, k, c});
+    S += k;
+  }
+  return out;
+}
+
+int run_transform(int field, const TwEntry* tw, uint32_t log_n, const uint4* d_src, uint4* d_dst, uint4* d_scratch,
+                  bool inverse, bool scale, const uint64_t* scale_val, cudaStream_t st) {
+  if (log_n == 0) {
+    // A length-1 transform has no stages; the inverse scale is by 1/1 = 1.
+    if (d_src != d_dst) ZCHECK(cudaMemcpyAsync(d_dst, d_src, 32, cudaMemcpyDeviceToDevice, st), "copy");
+    return ZNTT_OK;
+  }
+  auto passes = plan_passes(log_n);
+  const uint4* cur_src = d_src;
+  uint4* mid = (passes.size() == 1) ? d_dst : (d_dst != d_src ? d_dst : d_scratch);
+  if (!mid) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "in-place multi-pass transform needs scratch");
+  for (size_t p = 0; p < passes.size(); p++) {
+    const PassDesc& d = passes[p];
+    const bool last = p + 1 == passes.size();
+    PassParams pp;
+    std::memset(&pp, 0, sizeof(pp));
+    pp.src = cur_src;
+    pp.dst = last ? d_dst : mid;
+    pp.tw = tw->d_table;
+    pp.log_n = log_n;
+    pp.S = d.S;
+    pp.k = d.k;
+    pp.c = d.c;
+    pp.first = p == 0;
+    pp.inverse = inverse;
+    pp.tw0_one = tw->tw0_one;
+    pp.scale = last && scale;
+    if (pp.scale) std::memcpy(pp.scale_val, scale_val, 32);
+    const uint64_t tiles = (1ull << log_n) >> (d.k + d.c);
+    ZCHECK(launch_ntt_pass(field, pp, tiles, st), "ntt pass launch");
+    cur_src = pp.dst;
+  }
+  return ZNTT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// twiddle tables
+// ---------------------------------------------------------------------------
+
+static std::string table_key(int field, uint32_t log_n, const uint64_t* root) {
+  char buf[128];
+  std::snprintf(buf, sizeof(buf), "%d/%u/%016llx%016llx%016llx%016llx", field, log_n,
+                (unsigned long long)root[3], (unsigned long long)root[2], (unsigned long long)root[1],
+                (unsigned long long)root[0]);
+  return buf;
+}
+
+static size_t table_entries(uint32_t log_n) { return log_n == 0 ? 1 : ((size_t)1 << log_n) - 1; }
+
+static void free_entry(TwEntry* e) {
+  Context& c = ctx();
+  if (e->d_table) cudaFree(e->d_table);
+  c.all_tables.erase(std::remove(c.all_tables.begin(), c.all_tables.end(), e), c.all_tables.end());
+  for (auto it = c.tw_by_key.begin(); it != c.tw_by_key.end(); ++it) {
+    if (it->second == e) {
+      c.tw_by_key.erase(it);
+      break;
+    }
+  }
+  delete e;
+}
+
+// Keeps unreferenced root-derived tables up to the cache budget, oldest out first.
+static void evict_tables(size_t need) {
+  Context& c = ctx();
+  for (;;) {
+    size_t idle = 0;
+    TwEntry* oldest = nullptr;
+    for (TwEntry* e : c.all_tables) {
+      if (e->refs == 0) {
+        idle += e->bytes;
+        if (!oldest || e->last_use < oldest->last_use) oldest = e;
+      }
+    }
+    if (!oldest || idle + need <= c.table_cache_budget) return;
+    free_entry(oldest);
+  }
+}
+
+static int fill_table(TwEntry* e, cudaStream_t st) {
+  const HostField& F = host_field(e->field);
+  if (e->log_n == 0) return ZNTT_OK;
+  // pw[0][i] = root^i, pw[1][i] = root^(1024 i), pw[2][i] = root^(2^20 i), i < 1024.
+  std::vector<uint64_t> pw(3 * 1024 * 4);
+  uint64_t step[4];
+  std::memcpy(step, e->root, 32);
+  for (int t = 0; t < 3; t++) {
+    uint64_t cur[4];
+    std::memcpy(cur, F.one, 32);
+    for (int i = 0; i < 1024; i++) {
+      std::memcpy(&pw[(t * 1024 + i) * 4], cur, 32);
+      F.mul(cur, step, cur);
+    }
+    // step^1024 for the next level
+    uint64_t nxt[4];
+    F.pow_u64(step, 1024, nxt);
+    std::memcpy(step, nxt, 32);
+  }
+  PoolBuf d_pw;
+  int rc = d_pw.get(pw.size() * 8);
+  if (rc) return rc;
+  ZCHECK(cudaMemcpyAsync(d_pw.p, pw.data(), pw.size() * 8, cudaMemcpyHostToDevice, st), "twiddle powers upload");
+  ZCHECK(launch_twiddle_table(e->field, (const uint4*)d_pw.p, e->d_table, e->log_n, st), "twiddle kernel");
+  ZCHECK(cudaStreamSynchronize(st), "twiddle kernel");
+  return ZNTT_OK;
+}
+
+int acquire_table(int field, uint32_t log_n, const uint64_t* root, TwEntry** out) {
+  Context& c = ctx();
+  std::string key = table_key(field, log_n, root);
+  auto it = c.tw_by_key.find(key);
+  if (it != c.tw_by_key.end()) {
+    it->second->refs++;
+    it->second->last_use = ++c.clock;
+    *out = it->second;
+    return ZNTT_OK;
+  }
+  if (log_n > 31) return set_error(ZNTT_ERR_OUT_OF_MEMORY, "twiddle table larger than 2^31 entries");
+  TwEntry* e = new TwEntry();
+  e->field = field;
+  e->log_n = log_n;
+  std::memcpy(e->root, root, 32);
+  e->bytes = table_entries(log_n) * 32;
+  evict_tables(e->bytes);
+  cudaError_t ce = cudaMalloc((void**)&e->d_table, e->bytes);
+  if (ce == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    c.pool.trim();
+    evict_tables(c.table_cache_budget + 1);  // drop every idle table
+    ce = cudaMalloc((void**)&e->d_table, e->bytes);
+  }
+  if (ce != cudaSuccess) {
+    delete e;
+    return cuda_fail(ce, "twiddle table");
+  }
+  e->tw0_one = true;
+  int rc = fill_table(e, c.stream);
+  if (rc) {
+    cudaFree(e->d_table);
+    delete e;
+    return rc;
+  }
+  e->refs = 1;
+  e->last_use = ++c.clock;
+  c.all_tables.push_back(e);
+  c.tw_by_key[key] = e;
+  *out = e;
+  return ZNTT_OK;
+}
+
+void release_table(TwEntry* e) {
+  if (!e) return;
+  e->refs--;
+  if (e->refs <= 0) {
+    e->refs = 0;
+    if (e->foreign) free_entry(e);
+    else evict_tables(0);
+  }
+}
+
+// Builds a device table from a caller's host table that the library did not
+// make (or no longer recognises), with zig-ntt's exact per-stage semantics.
+static int upload_foreign_table(int field, uint32_t log_n, const zntt_stage* stages, TwEntry** out) {
+  Context& c = ctx();
+  const HostField& F = host_field(field);
+  TwEntry* e = new TwEntry();
+  e->field = field;
+  e->log_n = log_n;
+  e->foreign = true;
+  e->bytes = table_entries(log_n) * 32;
+  cudaError_t ce = cudaMalloc((void**)&e->d_table, e->bytes);
+  if (ce != cudaSuccess) {
+    delete e;
+    return cuda_fail(ce, "foreign twiddle table");
+  }
+  e->tw0_one = true;
+  for (uint32_t s = 0; s < log_n; s++) {
+    if (!F.is_one(stages[s].ptr)) e->tw0_one = false;
+    ce = cudaMemcpyAsync(e->d_table + 2 * (((size_t)1 << s) - 1), stages[s].ptr, ((size_t)1 << s) * 32,
+                         cudaMemcpyHostToDevice, c.stream);
+    if (ce != cudaSuccess) {
+      cudaFree(e->d_table);
+      delete e;
+      return cuda_fail(ce, "foreign twiddle upload");
+    }
+  }
+  e->refs = 1;
+  c.all_tables.push_back(e);
+  *out = e;
+  return ZNTT_OK;
+}
+
+static Registration* find_registration(int field, uint32_t log_n, const zntt_stage* stages) {
+  for (Registration& r : ctx().regs) {
+    if (r.field != field || r.log_n != log_n) continue;
+    bool same = true;
+    for (uint32_t s = 0; s < log_n && same; s++) same = r.stage_ptrs[s] == stages[s].ptr;
+    if (!same) continue;
+    // The table is const to its owner; still, re-check the entries that pin it.
+    for (uint32_t s = 0; s < log_n && same; s++) {
+      const size_t m = std::min<size_t>((size_t)1 << s, 2);
+      same = std::memcmp(stages[s].ptr, &r.probe[(2 * s) * 4], m * 32) == 0;
+    }
+    if (same) return &r;
+  }
+  return nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// host-data transform
+// ---------------------------------------------------------------------------
+
+static int transform_host(int field, uint64_t* data, uint32_t log_n, const TwEntry* tw, bool inverse, bool scale,
+                          const uint64_t* scale_val) {
+  Context& c = ctx();
+  const size_t n = (size_t)1 << log_n;
+  const size_t bytes = n * 32;
+  PoolBuf a, b;
+  int rc = a.get(bytes);
+  if (rc) return rc;
+  rc = b.get(bytes);
+  if (rc) return rc;
+  ZCHECK(cudaMemcpyAsync(a.p, data, bytes, cudaMemcpyHostToDevice, c.stream), "upload");
+  rc = run_transform(field, tw, log_n, (const uint4*)a.p, (uint4*)b.p, nullptr, inverse, scale, scale_val, c.stream);
+  if (rc) return rc;
+  ZCHECK(cudaMemcpyAsync(data, b.p, bytes, cudaMemcpyDeviceToHost, c.stream), "download");
+  ZCHECK(cudaStreamSynchronize(c.stream), "transform");
+  return ZNTT_OK;
+}
+
+static int check_field(int field) {
+  if (field != kBn254Fr && field != kBls12381Fr)
+    return set_error(ZNTT_ERR_UNSUPPORTED_FIELD, "unsupported field id " + std::to_string(field));
+  return ZNTT_OK;
+}
+
+static int check_init() {
+  if (ctx().device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
+  return ZNTT_OK;
+}
+
+// sizeFromLog and the length check (root.zig:33-36, 67-68).
+static int check_shape(size_t len, size_t log_n) {
+  if (log_n >= 64) return set_error(ZNTT_ERR_LOG_TOO_LARGE, "log_n >= 64");
+  if (len != ((size_t)1 << log_n)) return set_error(ZNTT_ERR_LENGTH_MISMATCH, "data.len != 2^log_n");
+  return ZNTT_OK;
+}
+
+static int check_fits(size_t log_n) {
+  if (log_n > 31) return set_error(ZNTT_ERR_OUT_OF_MEMORY, "transform larger than 2^31 elements");
+  return ZNTT_OK;
+}
+
+static void n_inverse(int field, uint32_t log_n, uint64_t* out) {
+  const HostField& F = host_field(field);
+  uint64_t nf[4];
+  F.from_u64((uint64_t)1 << log_n, nf);
+  F.inv(nf, out);
+}
+
+static int ntt_with_twiddles_impl(int field, uint64_t* data, size_t len, size_t log_n, const zntt_stage* stages,
+                                  size_t num_stages, bool inverse) {
+  clear_error();
+  int rc = check_field(field);
+  if (rc) return rc;
+  rc = check_shape(len, log_n);
+  if (rc) return rc;
+  if (num_stages != log_n) return set_error(ZNTT_ERR_INVALID_TWIDDLES, "twiddles.len != log_n");
+  if (num_stages && !stages) return set_error(ZNTT_ERR_INVALID_TWIDDLES, "null twiddle table");
+  for (size_t s = 0; s < num_stages; s++) {
+    if (stages[s].len != ((size_t)1 << s) || !stages[s].ptr)
+      return set_error(ZNTT_ERR_INVALID_TWIDDLES, "twiddle stage " + std::to_string(s) + " has the wrong length");
+  }
+  if (!data) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null data");
+  rc = check_fits(log_n);
+  if (rc) return rc;
+  rc = check_init();
+  if (rc) return rc;
+  if (log_n == 0) return ZNTT_OK;  // one element, no stage; the 1/n scale is by one
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  TwEntry* tw = nullptr;
+  bool foreign = false;
+  Registration* reg = find_registration(field, (uint32_t)log_n, stages);
+  if (reg) {
+    tw = reg->entry;
+    tw->last_use = ++c.clock;
+  } else {
+    rc = upload_foreign_table(field, (uint32_t)log_n, stages, &tw);
+    if (rc) return rc;
+    foreign = true;
+  }
+  uint64_t ninv[4];
+  if (inverse) n_inverse(field, (uint32_t)log_n, ninv);
+  rc = transform_host(field, data, (uint32_t)log_n, tw, inverse, inverse, ninv);
+  if (foreign) {
+    cudaStreamSynchronize(c.stream);
+    release_table(tw);
+  }
+  return rc;
+}
+
+static int ntt_root_impl(int field, uint64_t* data, size_t len, size_t log_n, const uint64_t* root, bool inverse) {
+  clear_error();
+  int rc = check_field(field);
+  if (rc) return rc;
+  rc = check_shape(len, log_n);
+  if (rc) return rc;
+  if (!data || !root) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
+  rc = check_fits(log_n);
+  if (rc) return rc;
+  rc = check_init();
+  if (rc) return rc;
+  if (log_n == 0) return ZNTT_OK;
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  const HostField& F = host_field(field);
+  // intt(root) is ntt(root.inv()) followed by the 1/n scale (root.zig:100-106).
+  uint64_t r[4];
+  if (inverse) F.inv(root, r);
+  else std::memcpy(r, root, 32);
+  TwEntry* tw = nullptr;
+  rc = acquire_table(field, (uint32_t)log_n, r, &tw);
+  if (rc) return rc;
+  uint64_t ninv[4];
+  if (inverse) n_inverse(field, (uint32_t)log_n, ninv);
+  rc = transform_host(field, data, (uint32_t)log_n, tw, false, inverse, ninv);
+  release_table(tw);
+  return rc;
+}
+
+}  // namespace zntt
+
+using namespace zntt;
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+int zntt_init(int device) {
+  clear_error();
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  if (c.device == device) return ZNTT_OK;
+  if (c.device >= 0) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "already initialised on another device");
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return set_error(ZNTT_ERR_DEVICE, "no CUDA device available");
+  }
+  if (device < 0 || device >= count) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "device id out of range");
+  ZCHECK(cudaSetDevice(device), "cudaSetDevice");
+  cudaDeviceProp prop;
+  ZCHECK(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+  if (prop.major != 10)
+    return set_error(ZNTT_ERR_DEVICE, std::string("kernels are built for sm_100a; device is ") + prop.name);
+  ZCHECK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  ZCHECK(configure_kernels(), "kernel attributes");
+  c.device = device;
+  return ZNTT_OK;
+}
+
+int zntt_shutdown(void) {
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  if (c.device < 0) return ZNTT_OK;
+  cudaSetDevice(c.device);
+  cudaStreamSynchronize(c.stream);
+  while (!c.all_tables.empty()) free_entry(c.all_tables.back());
+  c.regs.clear();
+  c.pool.trim();
+  cudaStreamDestroy(c.stream);
+  c.stream = nullptr;
+  c.device = -1;
+  return ZNTT_OK;
+}
+
+const char* zntt_last_error(void) { return g_last_error.c_str(); }
+
+int zntt_field_info(int field, uint64_t modulus[4], uint32_t* two_adicity) {
+  int rc = check_field(field);
+  if (rc) return rc;
+  const HostField& F = host_field(field);
+  if (modulus) std::memcpy(modulus, F.p, 32);
+  if (two_adicity) *two_adicity = F.two_adicity;
+  return ZNTT_OK;
+}
+
+int zntt_primitive_root(int field, uint32_t log_n, uint64_t root_out[4]) {
+  clear_error();
+  int rc = check_field(field);
+  if (rc) return rc;
+  const HostField& F = host_field(field);
+  if (log_n > F.two_adicity) return set_error(ZNTT_ERR_ORDER_TOO_LARGE, "log_n exceeds the two-adicity");
+  // z = first quadratic non-residue from 2: z^((p-1)/2) == -1 (Euler's criterion).
+  uint64_t half[4], pm1[4];
+  std::memcpy(pm1, F.p, 32);
+  pm1[0] -= 1;
+  for (int i = 0; i < 4; i++) half[i] = (pm1[i] >> 1) | (i < 3 ? (pm1[i + 1] << 63) : 0);
+  uint64_t minus_one[4];
+  {
+    // -1 = p - one
+    uint64_t br = 0;
+    for (int i = 0; i < 4; i++) {
+      u128 d = (u128)F.p[i] - F.one[i] - br;
+      minus_one[i] = (uint64_t)d;
+      br = (uint64_t)(d >> 127);
+    }
+  }
+  uint64_t z[4];
+  F.from_u64(2, z);
+  for (;;) {
+    uint64_t l[4];
+    F.pow_limbs(z, half, l);
+    if (std::memcmp(l, minus_one, 32) == 0) break;
+    F.add(z, F.one, z);
+  }
+  // exponent = odd_part << (two_adicity - log_n) = (p - 1) >> log_n
+  uint64_t e[4];
+  std::memcpy(e, pm1, 32);
+  for (uint32_t k = 0; k < log_n; k++)
+    for (int i = 0; i < 4; i++) e[i] = (e[i] >> 1) | (i < 3 ? (e[i + 1] << 63) : 0);
+  F.pow_limbs(z, e, root_out);
+  return ZNTT_OK;
+}
+
+int zntt_bit_reverse(uint64_t* data, size_t len) {
+  clear_error();
+  if (len == 0 || (len & (len - 1)) != 0) return set_error(ZNTT_ERR_INVALID_LENGTH, "length is 0 or not 2^k");
+  if (!data) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null data");
+  uint32_t log_n = (uint32_t)__builtin_ctzll(len);
+  int rc = check_fits(log_n);
+  if (rc) return rc;
+  rc = check_init();
+  if (rc) return rc;
+  if (len == 1) return ZNTT_OK;
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  PoolBuf a, b;
+  rc = a.get(len * 32);
+  if (rc) return rc;
+  rc = b.get(len * 32);
+  if (rc) return rc;
+  ZCHECK(cudaMemcpyAsync(a.p, data, len * 32, cudaMemcpyHostToDevice, c.stream), "upload");
+  ZCHECK(launch_bit_reverse((const uint4*)a.p, (uint4*)b.p, log_n, c.stream), "bit reverse");
+  ZCHECK(cudaMemcpyAsync(data, b.p, len * 32, cudaMemcpyDeviceToHost, c.stream), "download");
+  ZCHECK(cudaStreamSynchronize(c.stream), "bit reverse");
+  return ZNTT_OK;
+}
+
+int zntt_ntt(int field, uint64_t* data, size_t len, size_t log_n, const uint64_t root[4]) {
+  return ntt_root_impl(field, data, len, log_n, root, false);
+}
+
+int zntt_intt(int field, uint64_t* data, size_t len, size_t log_n, const uint64_t root[4]) {
+  return ntt_root_impl(field, data, len, log_n, root, true);
+}
+
+int zntt_precompute_twiddles(int field, size_t log_n, const uint64_t root[4], uint64_t* const* stage_out) {
+  clear_error();
+  int rc = check_field(field);
+  if (rc) return rc;
+  if (log_n >= 64) return set_error(ZNTT_ERR_LOG_TOO_LARGE, "log_n >= 64");
+  rc = check_fits(log_n);
+  if (rc) return rc;
+  if (log_n == 0) return ZNTT_OK;  // zero stages
+  if (!root || !stage_out) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
+  for (size_t s = 0; s < log_n; s++)
+    if (!stage_out[s]) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null stage pointer");
+  rc = check_init();
+  if (rc) return rc;
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  TwEntry* tw = nullptr;
+  rc = acquire_table(field, (uint32_t)log_n, root, &tw);
+  if (rc) return rc;
+  for (size_t s = 0; s < log_n; s++) {
+    cudaError_t e = cudaMemcpyAsync(stage_out[s], tw->d_table + 2 * (((size_t)1 << s) - 1), ((size_t)1 << s) * 32,
+                                    cudaMemcpyDeviceToHost, c.stream);
+    if (e != cudaSuccess) {
+      release_table(tw);
+      return cuda_fail(e, "twiddle download");
+    }
+  }
+  cudaError_t e = cudaStreamSynchronize(c.stream);
+  if (e != cudaSuccess) {
+    release_table(tw);
+    return cuda_fail(e, "twiddle download");
+  }
+  // Forget any stale registration at the same addresses, then register.
+  std::vector<zntt_stage> st(log_n);
+  for (size_t s = 0; s < log_n; s++) st[s] = {stage_out[s], (size_t)1 << s};
+  for (auto it = c.regs.begin(); it != c.regs.end();) {
+    bool same = it->field == field && it->log_n == log_n;
+    for (size_t s = 0; s < log_n && same; s++) same = it->stage_ptrs[s] == stage_out[s];
+    if (same) {
+      release_table(it->entry);
+      it = c.regs.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  Registration r;
+  r.field = field;
+  r.log_n = (uint32_t)log_n;
+  r.entry = tw;
+  r.probe.assign(2 * log_n * 4, 0);
+  for (size_t s = 0; s < log_n; s++) {
+    r.stage_ptrs.push_back(stage_out[s]);
+    const size_t m = std::min<size_t>((size_t)1 << s, 2);
+    std::memcpy(&r.probe[(2 * s) * 4], stage_out[s], m * 32);
+  }
+  c.regs.push_back(std::move(r));
+  return ZNTT_OK;
+}
+
+void zntt_free_twiddles(int field, const zntt_stage* stages, size_t num_stages) {
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  if (!stages || num_stages == 0) return;
+  for (auto it = c.regs.begin(); it != c.regs.end(); ++it) {
+    if (it->field != field || it->log_n != num_stages) continue;
+    bool same = true;
+    for (size_t s = 0; s < num_stages && same; s++) same = it->stage_ptrs[s] == stages[s].ptr;
+    if (same) {
+      release_table(it->entry);
+      c.regs.erase(it);
+      return;
+    }
+  }
+}
+
+int zntt_ntt_with_twiddles(int field, uint64_t* data, size_t len, size_t log_n, const zntt_stage* stages,
+                           size_t num_stages) {
+  return ntt_with_twiddles_impl(field, data, len, log_n, stages, num_stages, false);
+}
+
+int zntt_intt_with_twiddles(int field, uint64_t* data, size_t len, size_t log_n, const zntt_stage* stages,
+                            size_t num_stages) {
+  return ntt_with_twiddles_impl(field, data, len, log_n, stages, num_stages, true);
+}
+
+// ---- device-resident API ------------------------------------------------------
+
+struct zntt_twiddles {};  // opaque: a TwEntry behind the pointer
+
+int zntt_twiddles_acquire(int field, uint32_t log_n, const uint64_t root[4], zntt_twiddles** out) {
+  clear_error();
+  int rc = check_field(field);
+  if (rc) return rc;
+  if (!root || !out) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
+  rc = check_fits(log_n);
+  if (rc) return rc;
+  rc = check_init();
+  if (rc) return rc;
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  TwEntry* e = nullptr;
+  rc = acquire_table(field, log_n, root, &e);
+  if (rc) return rc;
+  *out = reinterpret_cast<zntt_twiddles*>(e);
+  return ZNTT_OK;
+}
+
+int zntt_twiddles_release(zntt_twiddles* tw) {
+  if (!tw) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null handle");
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  TwEntry* e = reinterpret_cast<TwEntry*>(tw);
+  if (std::find(c.all_tables.begin(), c.all_tables.end(), e) == c.all_tables.end())
+    return set_error(ZNTT_ERR_INVALID_ARGUMENT, "unknown twiddle handle");
+  release_table(e);
+  return ZNTT_OK;
+}
+
+int zntt_ntt_device(const zntt_twiddles* tw, const uint64_t* d_src, uint64_t* d_dst, uint64_t* d_scratch, int mode,
+                    void* stream) {
+  clear_error();
+  if (!tw || !d_src || !d_dst) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
+  if (mode != ZNTT_FORWARD && mode != ZNTT_INVERSE) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "unknown mode");
+  int rc = check_init();
+  if (rc) return rc;
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  const TwEntry* e = reinterpret_cast<const TwEntry*>(tw);
+  cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+  const bool inverse = mode == ZNTT_INVERSE;
+  uint64_t ninv[4];
+  if (inverse) n_inverse(e->field, e->log_n, ninv);
+  const bool need_scratch = d_src == d_dst && plan_passes(e->log_n).size() > 1;
+  if (need_scratch && !d_scratch) {
+    // Borrow a pool buffer; it returns to the pool only after the stream has
+    // finished with it, so wait here.
+    PoolBuf s;
+    rc = s.get(((size_t)1 << e->log_n) * 32);
+    if (rc) return rc;
+    rc = run_transform(e->field, e, e->log_n, (const uint4*)d_src, (uint4*)d_dst, (uint4*)s.p, inverse, inverse,
+                       ninv, st);
+    cudaError_t ce = cudaStreamSynchronize(st);
+    if (rc) return rc;
+    if (ce != cudaSuccess) return cuda_fail(ce, "transform");
+    return ZNTT_OK;
+  }
+  return run_transform(e->field, e, e->log_n, (const uint4*)d_src, (uint4*)d_dst, (uint4*)d_scratch, inverse,
+                       inverse, ninv, st);
+}
+
+int zntt_elementwise_device(int field, int op, const uint64_t* d_a, const uint64_t* d_b, uint64_t* d_out,
+                            size_t count, void* stream) {
+  clear_error();
+  int rc = check_field(field);
+  if (rc) return rc;
+  if (op < 0 || op > 3 || !d_a || !d_out || (op != 3 && !d_b))
+    return set_error(ZNTT_ERR_INVALID_ARGUMENT, "bad elementwise arguments");
+  rc = check_init();
+  if (rc) return rc;
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx().stream;
+  ZCHECK(launch_elementwise(field, op, (const uint4*)d_a, (const uint4*)d_b, (uint4*)d_out, count, st),
+         "elementwise");
+  return ZNTT_OK;
+}
+
+int zntt_probe_imad(double* per_second) {
+  clear_error();
+  int rc = check_init();
+  if (rc) return rc;
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+  PoolBuf sink;
+  rc = sink.get(64);
+  if (rc) return rc;
+  const int blocks = sms * 8, threads = 256;
+  const uint32_t iters = 4096;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  ZCHECK(launch_imad_probe((uint32_t*)sink.p, 64, blocks, threads, c.stream), "imad probe");  // warm-up
+  cudaEventRecord(e0, c.stream);
+  ZCHECK(launch_imad_probe((uint32_t*)sink.p, iters, blocks, threads, c.stream), "imad probe");
+  cudaEventRecord(e1, c.stream);
+  ZCHECK(cudaEventSynchronize(e1), "imad probe");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *per_second = (double)blocks * threads * iters * 32.0 / (ms * 1e-3);
+  return ZNTT_OK;
+}
+
+int zntt_probe_modmul(int field, double* per_second) {
+  clear_error();
+  int rc = check_field(field);
+  if (rc) return rc;
+  rc = check_init();
+  if (rc) return rc;
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+  PoolBuf sink;
+  rc = sink.get(64);
+  if (rc) return rc;
+  const int blocks = sms * 8, threads = 256;
+  const uint32_t iters = 512;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  ZCHECK(launch_modmul_probe(field, (uint4*)sink.p, 16, blocks, threads, c.stream), "modmul probe");
+  cudaEventRecord(e0, c.stream);
+  ZCHECK(launch_modmul_probe(field, (uint4*)sink.p, iters, blocks, threads, c.stream), "modmul probe");
+  cudaEventRecord(e1, c.stream);
+  ZCHECK(cudaEventSynchronize(e1), "modmul probe");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *per_second = (double)blocks * threads * iters * 2.0 / (ms * 1e-3);
+  return ZNTT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,88 @@
+// runtime.hpp -- library state shared by the C ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/zntt.h"
+#include "host_field.hpp"
+#include "kernels.cuh"
+
+namespace zntt {
+
+// A device twiddle table in zig-ntt's flat layout (stage s at entry 2^s - 1).
+struct TwEntry {
+  int field = 0;
+  uint32_t log_n = 0;
+  uint64_t root[4] = {0, 0, 0, 0};  // Montgomery form; the key of root-derived tables
+  uint4* d_table = nullptr;         // 2^log_n - 1 entries (one entry when log_n == 0)
+  size_t bytes = 0;
+  int refs = 0;                     // handles + registrations holding it
+  bool tw0_one = true;              // every stage's entry 0 equals one
+  bool foreign = false;             // uploaded from a caller's table, not derived from a root
+  uint64_t last_use = 0;
+};
+
+// A host table made by zntt_precompute_twiddles, recognised again by its stage
+// addresses; the first two entries of every stage are re-checked on use.
+struct Registration {
+  int field = 0;
+  uint32_t log_n = 0;
+  std::vector<const uint64_t*> stage_ptrs;
+  std::vector<uint64_t> probe;  // stage s entries 0 and 1 (when present), 4 limbs each
+  TwEntry* entry = nullptr;
+};
+
+// Pass structure of one transform size.
+struct PassDesc {
+  uint32_t S, k, c;
+};
+std::vector<PassDesc> plan_passes(uint32_t log_n);
+
+// Caching device allocator: freed buffers are kept by exact size for reuse.
+class BufferPool {
+ public:
+  cudaError_t acquire(size_t bytes, void** out);
+  void release(void* p, size_t bytes);
+  void trim();
+  size_t cached_bytes() const { return cached_; }
+
+ private:
+  std::multimap<size_t, void*> free_;
+  size_t cached_ = 0;
+};
+
+struct Context {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  std::recursive_mutex mu;
+  std::map<std::string, TwEntry*> tw_by_key;  // root-derived tables
+  std::vector<TwEntry*> all_tables;
+  std::vector<Registration> regs;
+  BufferPool pool;
+  uint64_t clock = 0;
+  size_t table_cache_budget = (size_t)16 << 30;  // unreferenced root tables kept up to this
+};
+
+Context& ctx();
+int set_error(int status, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+void clear_error();
+
+// Root-derived device table for (field, log_n, root); refs incremented.
+int acquire_table(int field, uint32_t log_n, const uint64_t* root, TwEntry** out);
+void release_table(TwEntry* e);
+
+// Runs the DIT network over 2^log_n device elements: d_src -> d_dst, with
+// d_scratch (2^log_n elements) used when d_src == d_dst and there are several
+// passes.  `inverse` selects the inttWithTwiddles twiddle mapping; `scale`
+// multiplies every output by `scale_val` (Montgomery form) after the last stage.
+int run_transform(int field, const TwEntry* tw, uint32_t log_n, const uint4* d_src, uint4* d_dst,
+                  uint4* d_scratch, bool inverse, bool scale, const uint64_t* scale_val, cudaStream_t st);
+
+}  // namespace zntt
