@@ -137,6 +137,9 @@ int zntt_elementwise_device(int field, int op, const uint64_t* d_a, const uint64
  * Throughput of the multiply pipe and of the field product on this device,
  * measured with CUDA events; used as the roofline denominator. */
 int zntt_probe_imad(double* imad_per_second);
+/* 32x32->64 multiply-adds (mad.wide.u32) per second: one 8x32-bit CIOS
+ * product needs 2*8*8 + 8 = 136 of them, so this / 136 is the modmul ceiling. */
+int zntt_probe_mul_wide(double* products_per_second);
 int zntt_probe_modmul(int field, double* modmul_per_second);
 
 #ifdef __cplusplus

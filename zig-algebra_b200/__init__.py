@@ -149,6 +149,7 @@ def lib():
         L.zntt_elementwise_device.argtypes = [i, i, vp, vp, vp, sz, vp]
         L.zntt_probe_imad.argtypes = [ctypes.POINTER(ctypes.c_double)]
         L.zntt_probe_modmul.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
+        L.zntt_probe_mul_wide.argtypes = [ctypes.POINTER(ctypes.c_double)]
         _lib = L
     return _lib
 
@@ -347,6 +348,14 @@ def probe_imad() -> float:
     _ensure_init()
     v = ctypes.c_double()
     _check(lib().zntt_probe_imad(ctypes.byref(v)))
+    return v.value
+
+
+def probe_mul_wide() -> float:
+    """32x32->64 multiply-adds per second (the modmul ceiling is this / 136)."""
+    _ensure_init()
+    v = ctypes.c_double()
+    _check(lib().zntt_probe_mul_wide(ctypes.byref(v)))
     return v.value
 
 

@@ -261,6 +261,30 @@ cudaError_t launch_imad_probe(uint32_t* sink, uint32_t iters, int blocks, int th
   return cudaGetLastError();
 }
 
+// Independent 32x32->64 multiply-adds (mad.wide.u32): the product the field
+// multiply needs 2N^2 + N = 136 of.  Eight accumulators per thread; each
+// iteration issues 8 products.
+__global__ void imad_wide_probe_kernel(unsigned long long* sink, uint32_t iters) {
+  const uint32_t a = threadIdx.x * 2654435761u + 1, b = blockIdx.x * 40503u + 7;
+  unsigned long long acc[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) acc[q] = a ^ (q * 977u);
+  for (uint32_t it = 0; it < iters; it++) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(acc[q]) : "r"(a + q), "r"(b));
+  }
+  unsigned long long x = 0;
+#pragma unroll
+  for (int q = 0; q < 8; q++) x ^= acc[q];
+  if (x == 0x9e3779b97f4a7c15ull) sink[0] = x;
+}
+
+cudaError_t launch_imad_wide_probe(unsigned long long* sink, uint32_t iters, int blocks, int threads,
+                                   cudaStream_t st) {
+  imad_wide_probe_kernel<<<blocks, threads, 0, st>>>(sink, iters);
+  return cudaGetLastError();
+}
+
 template <class F>
 __global__ void modmul_probe_kernel(uint4* sink, uint32_t iters) {
   fe x0, x1, y;

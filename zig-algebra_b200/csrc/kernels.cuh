@@ -59,6 +59,9 @@ cudaError_t launch_elementwise(int field, int op, const uint4* a, const uint4* b
 // Multiply-throughput probe: `iters` rounds of 8-long mad.lo/madc.hi carry
 // chains per thread; returns through `sink` so nothing is optimised away.
 cudaError_t launch_imad_probe(uint32_t* sink, uint32_t iters, int blocks, int threads, cudaStream_t st);
+// Independent 32x32->64 multiply-adds per thread (8 per iteration).
+cudaError_t launch_imad_wide_probe(unsigned long long* sink, uint32_t iters, int blocks, int threads,
+                                   cudaStream_t st);
 // Independent modular products per thread, to time the field multiply alone.
 cudaError_t launch_modmul_probe(int field, uint4* sink, uint32_t iters, int blocks, int threads,
                                 cudaStream_t st);

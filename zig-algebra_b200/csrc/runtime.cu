@@ -780,6 +780,35 @@ int zntt_probe_imad(double* per_second) {
   return ZNTT_OK;
 }
 
+int zntt_probe_mul_wide(double* per_second) {
+  clear_error();
+  int rc = check_init();
+  if (rc) return rc;
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+  PoolBuf sink;
+  rc = sink.get(64);
+  if (rc) return rc;
+  const int blocks = sms * 8, threads = 256;
+  const uint32_t iters = 8192;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  ZCHECK(launch_imad_wide_probe((unsigned long long*)sink.p, 64, blocks, threads, c.stream), "wide probe");
+  cudaEventRecord(e0, c.stream);
+  ZCHECK(launch_imad_wide_probe((unsigned long long*)sink.p, iters, blocks, threads, c.stream), "wide probe");
+  cudaEventRecord(e1, c.stream);
+  ZCHECK(cudaEventSynchronize(e1), "wide probe");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *per_second = (double)blocks * threads * iters * 8.0 / (ms * 1e-3);
+  return ZNTT_OK;
+}
+
 int zntt_probe_modmul(int field, double* per_second) {
   clear_error();
   int rc = check_field(field);
