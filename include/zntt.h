@@ -135,7 +135,10 @@ int zntt_elementwise_device(int field, int op, const uint64_t* d_a, const uint64
 
 /* ---- roofline probes ---------------------------------------------------------
  * Throughput of the multiply pipe and of the field product on this device,
- * measured with CUDA events; used as the roofline denominator. */
+ * measured with CUDA events.  zntt_probe_imad counts dependent 32-bit
+ * multiply-adds (mad.lo.u32), the multiply pipe's unit of issue; a full
+ * 32x32->64 product takes two, so an 8x32-bit CIOS product (136 products)
+ * takes 272 and imad_per_second / 272 is the modmul roofline. */
 int zntt_probe_imad(double* imad_per_second);
 /* 32x32->64 multiply-adds (mad.wide.u32) per second: one 8x32-bit CIOS
  * product needs 2*8*8 + 8 = 136 of them, so this / 136 is the modmul ceiling. */

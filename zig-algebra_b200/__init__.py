@@ -28,7 +28,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libzntt_cuda.so")
+LIB_PATH = os.environ.get("ZNTT_LIB") or os.path.join(HERE, "libzntt_cuda.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "zntt.h")
 
 

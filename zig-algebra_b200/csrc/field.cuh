@@ -27,8 +27,15 @@
 
 namespace zntt {
 
+// kRed selects the reduction step of the field product:
+//   0  generic: m = T0 * N0, then m * p with 8 products per row
+//   1  BN254-Fr: N0 = -(2^28 + 1) and p0 = 2^32 - 2^28 + 1, so m and m * p0
+//      come from shifts and adds (7 products per row instead of 9)
+//   2  BLS12-381-Fr: N0 = -1, p0 = 1 and p1 = 2^32 - 1, so m, m * p0 and
+//      m * p1 come from adds (6 products per row instead of 9)
 struct Bn254Fr {
   static constexpr int kId = 0;
+  static constexpr int kRed = 1;
   static constexpr uint32_t P0 = 0xf0000001u, P1 = 0x43e1f593u, P2 = 0x79b97091u, P3 = 0x2833e848u,
                             P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
   static constexpr uint32_t N0 = 0xefffffffu;  // -p^-1 mod 2^32
@@ -42,6 +49,7 @@ struct Bn254Fr {
 
 struct Bls12381Fr {
   static constexpr int kId = 1;
+  static constexpr int kRed = 2;
   static constexpr uint32_t P0 = 0x00000001u, P1 = 0xffffffffu, P2 = 0xfffe5bfeu, P3 = 0x53bda402u,
                             P4 = 0x09a1d805u, P5 = 0x3339d808u, P6 = 0x299d7d48u, P7 = 0x73eda753u;
   static constexpr uint32_t N0 = 0xffffffffu;
@@ -222,30 +230,87 @@ __device__ __forceinline__ void cios_row(uint32_t (&T)[9], const fe& a, uint32_t
       "mul.hi.u32 %7, %11, %12;"
       : "=r"(U0), "=r"(U1), "=r"(U2), "=r"(U3), "=r"(U4), "=r"(U5), "=r"(U6), "=r"(U7)
       : "r"(a.v[1]), "r"(a.v[3]), "r"(a.v[5]), "r"(a.v[7]), "r"(w));
-  m = T[0] * F::N0;
-  asm("mad.lo.cc.u32  %0, %9, %10, %0;\n\t"
-      "madc.hi.cc.u32 %1, %9, %10, %1;\n\t"
-      "madc.lo.cc.u32 %2, %9, %11, %2;\n\t"
-      "madc.hi.cc.u32 %3, %9, %11, %3;\n\t"
-      "madc.lo.cc.u32 %4, %9, %12, %4;\n\t"
-      "madc.hi.cc.u32 %5, %9, %12, %5;\n\t"
-      "madc.lo.cc.u32 %6, %9, %13, %6;\n\t"
-      "madc.hi.cc.u32 %7, %9, %13, %7;\n\t"
-      "addc.u32       %8, %8, 0;"
-      : "+r"(T[0]), "+r"(T[1]), "+r"(T[2]), "+r"(T[3]), "+r"(T[4]), "+r"(T[5]), "+r"(T[6]),
-        "+r"(T[7]), "+r"(T[8])
-      : "r"(m), "n"(F::P0), "n"(F::P2), "n"(F::P4), "n"(F::P6));
-  asm("mad.lo.cc.u32  %0, %9, %10, %0;\n\t"
-      "madc.hi.cc.u32 %1, %9, %10, %1;\n\t"
-      "madc.lo.cc.u32 %2, %9, %11, %2;\n\t"
-      "madc.hi.cc.u32 %3, %9, %11, %3;\n\t"
-      "madc.lo.cc.u32 %4, %9, %12, %4;\n\t"
-      "madc.hi.cc.u32 %5, %9, %12, %5;\n\t"
-      "madc.lo.cc.u32 %6, %9, %13, %6;\n\t"
-      "madc.hi.cc.u32 %7, %9, %13, %7;\n\t"
-      "addc.u32       %8, 0, 0;"
-      : "+r"(U0), "+r"(U1), "+r"(U2), "+r"(U3), "+r"(U4), "+r"(U5), "+r"(U6), "+r"(U7), "=r"(U8)
-      : "r"(m), "n"(F::P1), "n"(F::P3), "n"(F::P5), "n"(F::P7));
+  if constexpr (F::kRed == 1) {
+    // m = T0 * N0 = -(T0 + T0 * 2^28) mod 2^32.
+    m = 0u - T[0] - (T[0] << 28);
+    // Words 0 and 1 of T + m * p0 with p0 = 2^32 - D/m, D = m * (2^28 - 1):
+    // word 0 becomes zero and word 1 gains m - floor(D / 2^32) (the carry out
+    // of word 0 and the rounding of the high half cancel).
+    // floor(D / 2^32) = (m >> 4) - [((m << 28) mod 2^32) < m].
+    uint32_t a;
+    asm("{\n\t.reg .u32 x, d;\n\t"
+        "shl.b32     x, %1, 28;\n\t"
+        "sub.cc.u32  x, x, %1;\n\t"
+        "shr.b32     d, %1, 4;\n\t"
+        "subc.u32    d, d, 0;\n\t"
+        "sub.u32     %0, %1, d;\n\t}"
+        : "=r"(a)
+        : "r"(m));
+    asm("add.cc.u32     %0, %0, %8;\n\t"
+        "madc.lo.cc.u32 %1, %9, %10, %1;\n\t"
+        "madc.hi.cc.u32 %2, %9, %10, %2;\n\t"
+        "madc.lo.cc.u32 %3, %9, %11, %3;\n\t"
+        "madc.hi.cc.u32 %4, %9, %11, %4;\n\t"
+        "madc.lo.cc.u32 %5, %9, %12, %5;\n\t"
+        "madc.hi.cc.u32 %6, %9, %12, %6;\n\t"
+        "addc.u32       %7, %7, 0;"
+        : "+r"(T[1]), "+r"(T[2]), "+r"(T[3]), "+r"(T[4]), "+r"(T[5]), "+r"(T[6]), "+r"(T[7]), "+r"(T[8])
+        : "r"(a), "r"(m), "n"(F::P2), "n"(F::P4), "n"(F::P6));
+  } else if constexpr (F::kRed == 2) {
+    // m = -T0 mod 2^32.  With p0 = 1: T0 + m = 0 with carry [T0 != 0] and a
+    // zero high half.  With p1 = 2^32 - 1: m * p1 = (m - [m != 0]) * 2^32 +
+    // (-m mod 2^32) and -m mod 2^32 = T0.
+    m = 0u - T[0];
+    const uint32_t c0 = T[0] != 0u ? 1u : 0u;
+    asm("add.cc.u32     %0, %0, %8;\n\t"
+        "madc.lo.cc.u32 %1, %9, %10, %1;\n\t"
+        "madc.hi.cc.u32 %2, %9, %10, %2;\n\t"
+        "madc.lo.cc.u32 %3, %9, %11, %3;\n\t"
+        "madc.hi.cc.u32 %4, %9, %11, %4;\n\t"
+        "madc.lo.cc.u32 %5, %9, %12, %5;\n\t"
+        "madc.hi.cc.u32 %6, %9, %12, %6;\n\t"
+        "addc.u32       %7, %7, 0;"
+        : "+r"(T[1]), "+r"(T[2]), "+r"(T[3]), "+r"(T[4]), "+r"(T[5]), "+r"(T[6]), "+r"(T[7]), "+r"(T[8])
+        : "r"(c0), "r"(m), "n"(F::P2), "n"(F::P4), "n"(F::P6));
+    asm("add.cc.u32     %0, %0, %9;\n\t"
+        "addc.cc.u32    %1, %1, %10;\n\t"
+        "madc.lo.cc.u32 %2, %11, %12, %2;\n\t"
+        "madc.hi.cc.u32 %3, %11, %12, %3;\n\t"
+        "madc.lo.cc.u32 %4, %11, %13, %4;\n\t"
+        "madc.hi.cc.u32 %5, %11, %13, %5;\n\t"
+        "madc.lo.cc.u32 %6, %11, %14, %6;\n\t"
+        "madc.hi.cc.u32 %7, %11, %14, %7;\n\t"
+        "addc.u32       %8, 0, 0;"
+        : "+r"(U0), "+r"(U1), "+r"(U2), "+r"(U3), "+r"(U4), "+r"(U5), "+r"(U6), "+r"(U7), "=r"(U8)
+        : "r"(T[0]), "r"(m - c0), "r"(m), "n"(F::P3), "n"(F::P5), "n"(F::P7));
+  } else {
+    m = T[0] * F::N0;
+    asm("mad.lo.cc.u32  %0, %9, %10, %0;\n\t"
+        "madc.hi.cc.u32 %1, %9, %10, %1;\n\t"
+        "madc.lo.cc.u32 %2, %9, %11, %2;\n\t"
+        "madc.hi.cc.u32 %3, %9, %11, %3;\n\t"
+        "madc.lo.cc.u32 %4, %9, %12, %4;\n\t"
+        "madc.hi.cc.u32 %5, %9, %12, %5;\n\t"
+        "madc.lo.cc.u32 %6, %9, %13, %6;\n\t"
+        "madc.hi.cc.u32 %7, %9, %13, %7;\n\t"
+        "addc.u32       %8, %8, 0;"
+        : "+r"(T[0]), "+r"(T[1]), "+r"(T[2]), "+r"(T[3]), "+r"(T[4]), "+r"(T[5]), "+r"(T[6]),
+          "+r"(T[7]), "+r"(T[8])
+        : "r"(m), "n"(F::P0), "n"(F::P2), "n"(F::P4), "n"(F::P6));
+  }
+  if constexpr (F::kRed != 2) {
+    asm("mad.lo.cc.u32  %0, %9, %10, %0;\n\t"
+        "madc.hi.cc.u32 %1, %9, %10, %1;\n\t"
+        "madc.lo.cc.u32 %2, %9, %11, %2;\n\t"
+        "madc.hi.cc.u32 %3, %9, %11, %3;\n\t"
+        "madc.lo.cc.u32 %4, %9, %12, %4;\n\t"
+        "madc.hi.cc.u32 %5, %9, %12, %5;\n\t"
+        "madc.lo.cc.u32 %6, %9, %13, %6;\n\t"
+        "madc.hi.cc.u32 %7, %9, %13, %7;\n\t"
+        "addc.u32       %8, 0, 0;"
+        : "+r"(U0), "+r"(U1), "+r"(U2), "+r"(U3), "+r"(U4), "+r"(U5), "+r"(U6), "+r"(U7), "=r"(U8)
+        : "r"(m), "n"(F::P1), "n"(F::P3), "n"(F::P5), "n"(F::P7));
+  }
   // T[0] is now zero: shift down one word and fold U in.  The result is below
   // 2p < 2^256, so the ninth word of the sum is zero and is not kept.
   asm("add.cc.u32  %0, %0, %8;\n\t"

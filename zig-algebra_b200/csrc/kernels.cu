@@ -31,8 +31,33 @@ __device__ __forceinline__ uint32_t rev_bits(uint32_t x, uint32_t bits) {
   return bits == 0 ? 0u : (__brev(x) >> (32 - bits));
 }
 
+// Twiddle of global stage s (1-based) for butterfly index jg, with the
+// forward (tw[s-1][jg]) or inttWithTwiddles (1 or -tw[s-1][2^(s-1) - jg])
+// mapping.  `stw` points at tw[s-1]; returns false when the factor is one
+// and the multiply can be skipped.
 template <class F>
-__global__ void __launch_bounds__(kPassThreads, 3) ntt_pass_kernel(PassParams pp) {
+__device__ __forceinline__ bool twiddle(const PassParams& pp, const uint4* stw, uint64_t half_g, uint64_t jg,
+                                        fe& w) {
+  if (jg == 0 && (pp.inverse | pp.tw0_one)) return false;
+  if (!pp.inverse) {
+    w = fe_load_nc(stw + (jg << 1));
+  } else {
+    w = fe_neg<F>(fe_load_nc(stw + ((half_g - jg) << 1)));
+  }
+  return true;
+}
+
+// u, v -> u + w v, u - w v
+template <class F>
+__device__ __forceinline__ void butterfly(fe& u, fe& v, bool mul, const fe& w) {
+  const fe t = mul ? fe_mul<F>(w, v) : v;
+  v = fe_sub<F>(u, t);
+  u = fe_add<F>(u, t);
+}
+
+template <class F, int LOG_TILE, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) ntt_pass_kernel(PassParams pp) {
+  constexpr uint32_t TILE_MAX = 1u << LOG_TILE;
   extern __shared__ uint4 sm[];
   const uint32_t k = pp.k, c = pp.c, C = 1u << c;
   const uint32_t tile = 1u << (k + c);
@@ -47,51 +72,89 @@ __global__ void __launch_bounds__(kPassThreads, 3) ntt_pass_kernel(PassParams pp
     hi_base = (blk >> mlog) << (pp.S + k);
     m0 = (blk & ((1ull << mlog) - 1)) << c;
   }
-  const uint32_t xcols_log = pp.log_n - k;  // first pass: columns of the 2^k x 2^(L-k) view
+  const uint32_t xcols_log = pp.log_n - k;
 
-  // Load: column-fastest so each tile row is one contiguous run of C elements.
-  for (uint32_t idx = tid; idx < 2 * tile; idx += kPassThreads) {
-    const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
-    uint64_t g;
-    uint32_t t;
-    if (pp.first) {
-      g = ((uint64_t)row << xcols_log) + col0 + col;
-      t = rev_bits(row, k);
-    } else {
-      g = hi_base + ((uint64_t)row << pp.S) + m0 + col;
-      t = row;
+  // ---- load: column-fastest, 16-byte halves ----
+#pragma unroll
+  for (uint32_t q = 0; q < 2 * TILE_MAX / THREADS; q++) {
+    const uint32_t idx = tid + q * THREADS;
+    if (idx < 2 * tile) {
+      const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
+      uint64_t g;
+      uint32_t t;
+      if (pp.first) {
+        g = ((uint64_t)row << xcols_log) + col0 + col;
+        t = rev_bits(row, k);
+      } else {
+        g = hi_base + ((uint64_t)row << pp.S) + m0 + col;
+        t = row;
+      }
+      sm[h * TILE_MAX + ((t << c) | col)] = pp.src[(g << 1) | h];
     }
-    sm[h * kTileMax + t * C + col] = pp.src[2 * g + h];
   }
   __syncthreads();
 
-  for (uint32_t i = 1; i <= k; i++) {
-    const uint32_t halfm = 1u << (i - 1);
-    const uint32_t s = pp.S + i;                      // global 1-based stage
-    const uint64_t half_g = 1ull << (s - 1);          // butterflies per block = stage length
-    const uint4* stw = pp.tw + 2 * (half_g - 1);      // tw[s-1]
-    for (uint32_t b = tid; b < tile / 2; b += kPassThreads) {
-      const uint32_t col = b & (C - 1), bb = b >> c;
-      const uint32_t j = bb & (halfm - 1);
-      const uint32_t t0 = ((bb >> (i - 1)) << i) | j, t1 = t0 + halfm;
-      const uint64_t jg = pp.first ? (uint64_t)j : (((uint64_t)j << pp.S) + m0 + col);
-      const uint32_t e0 = t0 * C + col, e1 = t1 * C + col;
-      fe u = sm_load(sm, e0);
-      fe v = sm_load(sm, e1);
-      fe tv;
-      if (jg == 0 && (pp.inverse | pp.tw0_one)) {
-        tv = v;
-      } else {
-        fe w;
-        if (!pp.inverse) {
-          w = fe_load_nc(stw + 2 * jg);
-        } else {
-          w = fe_neg<F>(fe_load_nc(stw + 2 * (half_g - jg)));
-        }
-        tv = fe_mul<F>(w, v);
+  uint32_t i = 1;
+  // ---- an odd stage count starts with one radix-2 stage ----
+  if (k & 1) {
+    const uint64_t half_g = 1ull << pp.S;  // stage S+1
+    const uint4* stw = pp.tw + ((half_g - 1) << 1);
+#pragma unroll
+    for (uint32_t q = 0; q < TILE_MAX / 2 / THREADS; q++) {
+      const uint32_t b = tid + q * THREADS;
+      if (b < tile / 2) {
+        const uint32_t col = b & (C - 1), t0 = (b >> c) << 1;  // half = 1: j = 0
+        const uint64_t jg = pp.first ? 0 : m0 + col;
+        const uint32_t e0 = (t0 << c) | col, e1 = e0 + C;
+        fe u = sm_load(sm, e0), v = sm_load(sm, e1), w;
+        const bool mul = twiddle<F>(pp, stw, half_g, jg, w);
+        butterfly<F>(u, v, mul, w);
+        sm_store(sm, e0, u);
+        sm_store(sm, e1, v);
       }
-      sm_store(sm, e0, fe_add<F>(u, tv));
-      sm_store(sm, e1, fe_sub<F>(u, tv));
+    }
+    __syncthreads();
+    i = 2;
+  }
+
+  // ---- radix-4 groups: stages i and i+1 on four elements in registers ----
+  for (; i < k; i += 2) {
+    const uint32_t h = 1u << (i - 1);
+    const uint64_t half1 = 1ull << (pp.S + i - 1);  // stage S+i
+    const uint64_t half2 = half1 << 1;              // stage S+i+1
+    const uint4* stw1 = pp.tw + ((half1 - 1) << 1);
+    const uint4* stw2 = pp.tw + ((half2 - 1) << 1);
+#pragma unroll
+    for (uint32_t q = 0; q < TILE_MAX / 4 / THREADS; q++) {
+      const uint32_t ga = tid + q * THREADS;
+      if (ga < tile / 4) {
+        const uint32_t col = ga & (C - 1), g = ga >> c;
+        const uint32_t j = g & (h - 1);
+        const uint32_t t0 = ((g >> (i - 1)) << (i + 1)) | j;
+        const uint32_t e0 = (t0 << c) | col, eh = h << c;
+        uint64_t jg1, jg3;
+        if (pp.first) {
+          jg1 = j;
+          jg3 = j + h;
+        } else {
+          jg1 = ((uint64_t)j << pp.S) + m0 + col;
+          jg3 = jg1 + ((uint64_t)h << pp.S);
+        }
+        fe w1, w2, w3;
+        const bool m1 = twiddle<F>(pp, stw1, half1, jg1, w1);
+        const bool m2 = twiddle<F>(pp, stw2, half2, jg1, w2);
+        const bool m3 = twiddle<F>(pp, stw2, half2, jg3, w3);
+        fe x0 = sm_load(sm, e0), x1 = sm_load(sm, e0 + eh), x2 = sm_load(sm, e0 + 2 * eh),
+           x3 = sm_load(sm, e0 + 3 * eh);
+        butterfly<F>(x0, x1, m1, w1);
+        butterfly<F>(x2, x3, m1, w1);
+        butterfly<F>(x0, x2, m2, w2);
+        butterfly<F>(x1, x3, m3, w3);
+        sm_store(sm, e0, x0);
+        sm_store(sm, e0 + eh, x1);
+        sm_store(sm, e0 + 2 * eh, x2);
+        sm_store(sm, e0 + 3 * eh, x3);
+      }
     }
     __syncthreads();
   }
@@ -100,36 +163,46 @@ __global__ void __launch_bounds__(kPassThreads, 3) ntt_pass_kernel(PassParams pp
     fe sc;
 #pragma unroll
     for (int q = 0; q < 8; q++) sc.v[q] = pp.scale_val[q];
-    for (uint32_t e = tid; e < tile; e += kPassThreads) sm_store(sm, e, fe_mul<F>(sm_load(sm, e), sc));
+#pragma unroll
+    for (uint32_t q = 0; q < TILE_MAX / THREADS; q++) {
+      const uint32_t e = tid + q * THREADS;
+      if (e < tile) sm_store(sm, e, fe_mul<F>(sm_load(sm, e), sc));
+    }
     __syncthreads();
   }
 
-  for (uint32_t idx = tid; idx < 2 * tile; idx += kPassThreads) {
-    const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
-    uint64_t g;
-    if (pp.first) {
-      g = ((uint64_t)rev_bits((uint32_t)(col0 + col), xcols_log) << k) + row;
-    } else {
-      g = hi_base + ((uint64_t)row << pp.S) + m0 + col;
+  // ---- store ----
+#pragma unroll
+  for (uint32_t q = 0; q < 2 * TILE_MAX / THREADS; q++) {
+    const uint32_t idx = tid + q * THREADS;
+    if (idx < 2 * tile) {
+      const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
+      uint64_t g;
+      if (pp.first) {
+        g = ((uint64_t)rev_bits((uint32_t)(col0 + col), xcols_log) << k) + row;
+      } else {
+        g = hi_base + ((uint64_t)row << pp.S) + m0 + col;
+      }
+      pp.dst[(g << 1) | h] = sm[h * TILE_MAX + ((row << c) | col)];
     }
-    pp.dst[2 * g + h] = sm[h * kTileMax + row * C + col];
   }
 }
 
+#define ZNTT_PASS(F) ntt_pass_kernel<F, kLogTile, kPassThreads, kPassMinBlocks>
+
 cudaError_t configure_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(ntt_pass_kernel<Bn254Fr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(ZNTT_PASS(Bn254Fr), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        kPassSmemBytes);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(ntt_pass_kernel<Bls12381Fr>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              kPassSmemBytes);
+  return cudaFuncSetAttribute(ZNTT_PASS(Bls12381Fr), cudaFuncAttributeMaxDynamicSharedMemorySize, kPassSmemBytes);
 }
 
 cudaError_t launch_ntt_pass(int field, const PassParams& pp, uint64_t num_tiles, cudaStream_t st) {
   dim3 grid((unsigned)num_tiles);
   if (field == kBn254Fr)
-    ntt_pass_kernel<Bn254Fr><<<grid, kPassThreads, kPassSmemBytes, st>>>(pp);
+    ZNTT_PASS(Bn254Fr)<<<grid, kPassThreads, kPassSmemBytes, st>>>(pp);
   else
-    ntt_pass_kernel<Bls12381Fr><<<grid, kPassThreads, kPassSmemBytes, st>>>(pp);
+    ZNTT_PASS(Bls12381Fr)<<<grid, kPassThreads, kPassSmemBytes, st>>>(pp);
   return cudaGetLastError();
 }
 
@@ -222,38 +295,24 @@ cudaError_t launch_elementwise(int field, int op, const uint4* a, const uint4* b
 // Throughput probes for the roofline denominator
 // ---------------------------------------------------------------------------
 
-// Four independent 8-multiply carry chains per iteration (mad.lo.cc/madc.hi.cc
-// pairs, the instruction mix of the field multiply).  Each iteration issues
-// 4 x 8 = 32 multiply-class instructions.
+// 32-bit multiply-adds (mad.lo.u32), the multiply pipe's unit of issue: a
+// full 32x32->64 product costs two of them (lo and hi), so one 8x32-bit CIOS
+// field product (136 products) costs 272.  Each multiply takes the previous
+// result as its multiplicand, so nothing can be hoisted; eight independent
+// chains per thread.  Each iteration issues 8 multiply-adds.
 __global__ void imad_probe_kernel(uint32_t* sink, uint32_t iters) {
-  uint32_t a = threadIdx.x * 2654435761u + 1, b = blockIdx.x * 40503u + 7;
-  uint32_t t[4][5];
+  const uint32_t b = (blockIdx.x * 40503u + threadIdx.x * 2654435761u) | 1u;
+  uint32_t acc[8];
 #pragma unroll
-  for (int q = 0; q < 4; q++)
-#pragma unroll
-    for (int r = 0; r < 5; r++) t[q][r] = a ^ (q * 5 + r);
+  for (int q = 0; q < 8; q++) acc[q] = threadIdx.x * 977u + q * 131u + 1u;
   for (uint32_t it = 0; it < iters; it++) {
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      asm volatile(
-          "mad.lo.cc.u32  %0, %5, %6, %0;\n\t"
-          "madc.hi.cc.u32 %1, %5, %6, %1;\n\t"
-          "madc.lo.cc.u32 %2, %5, %6, %2;\n\t"
-          "madc.hi.cc.u32 %3, %5, %6, %3;\n\t"
-          "madc.lo.cc.u32 %4, %5, %6, %4;\n\t"
-          "madc.hi.cc.u32 %0, %5, %6, %0;\n\t"
-          "madc.lo.cc.u32 %1, %5, %6, %1;\n\t"
-          "madc.hi.u32    %2, %5, %6, %2;"
-          : "+r"(t[q][0]), "+r"(t[q][1]), "+r"(t[q][2]), "+r"(t[q][3]), "+r"(t[q][4])
-          : "r"(a + q), "r"(b));
-    }
+    for (int q = 0; q < 8; q++) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(acc[q]) : "r"(b), "r"(q * 7u + 1u));
   }
-  uint32_t acc = 0;
+  uint32_t x = 0;
 #pragma unroll
-  for (int q = 0; q < 4; q++)
-#pragma unroll
-    for (int r = 0; r < 5; r++) acc ^= t[q][r];
-  if (acc == 0x9e3779b9u) sink[0] = acc;  // practically never; keeps the chains live
+  for (int q = 0; q < 8; q++) x ^= acc[q];
+  if (x == 0x9e3779b9u) sink[0] = x;
 }
 
 cudaError_t launch_imad_probe(uint32_t* sink, uint32_t iters, int blocks, int threads, cudaStream_t st) {
@@ -261,17 +320,22 @@ cudaError_t launch_imad_probe(uint32_t* sink, uint32_t iters, int blocks, int th
   return cudaGetLastError();
 }
 
-// Independent 32x32->64 multiply-adds (mad.wide.u32): the product the field
-// multiply needs 2N^2 + N = 136 of.  Eight accumulators per thread; each
-// iteration issues 8 products.
+// Full 32x32->64 products (mad.wide.u32), the unit the field multiply needs
+// 2N^2 + N = 136 of.  Each product's multiplicand is the low word of the
+// previous result, so the product cannot be hoisted out of the loop; eight
+// independent chains per thread keep the multiply pipe fed.  Each iteration
+// issues 8 products.
 __global__ void imad_wide_probe_kernel(unsigned long long* sink, uint32_t iters) {
-  const uint32_t a = threadIdx.x * 2654435761u + 1, b = blockIdx.x * 40503u + 7;
+  const uint32_t b = (blockIdx.x * 40503u + threadIdx.x * 2654435761u) | 1u;
   unsigned long long acc[8];
 #pragma unroll
-  for (int q = 0; q < 8; q++) acc[q] = a ^ (q * 977u);
+  for (int q = 0; q < 8; q++) acc[q] = (threadIdx.x * 977u + q * 131u) | 1u;
   for (uint32_t it = 0; it < iters; it++) {
 #pragma unroll
-    for (int q = 0; q < 8; q++) asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(acc[q]) : "r"(a + q), "r"(b));
+    for (int q = 0; q < 8; q++) {
+      const uint32_t lo = (uint32_t)acc[q];
+      asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(acc[q]) : "r"(lo), "r"(b));
+    }
   }
   unsigned long long x = 0;
 #pragma unroll
@@ -292,7 +356,7 @@ __global__ void modmul_probe_kernel(uint4* sink, uint32_t iters) {
   for (int q = 0; q < 8; q++) {
     x0.v[q] = (threadIdx.x * 2654435761u + q) & 0x0fffffff;
     x1.v[q] = (blockIdx.x * 40503u + q * 7) & 0x0fffffff;
-    y.v[q] = (q * 0x01000193u + 3) & 0x0fffffff;
+    y.v[q] = (threadIdx.x * 0x01000193u + q * 3 + 5) & 0x0fffffff;
   }
   for (uint32_t it = 0; it < iters; it++) {
     x0 = fe_mul<F>(x0, y);

@@ -35,8 +35,19 @@ struct PassParams {
   uint32_t scale_val[8];
 };
 
-constexpr int kPassThreads = 256;
-constexpr int kLogTile = 11;                      // 2048 elements = 64 KiB of shared memory
+// Pass kernel shape (overridable at build time for tuning sweeps).
+#ifndef ZNTT_PASS_THREADS
+#define ZNTT_PASS_THREADS 256
+#endif
+#ifndef ZNTT_PASS_MIN_BLOCKS
+#define ZNTT_PASS_MIN_BLOCKS 3
+#endif
+#ifndef ZNTT_LOG_TILE
+#define ZNTT_LOG_TILE 11
+#endif
+constexpr int kPassThreads = ZNTT_PASS_THREADS;
+constexpr int kPassMinBlocks = ZNTT_PASS_MIN_BLOCKS;
+constexpr int kLogTile = ZNTT_LOG_TILE;                  // 2^11 elements = 64 KiB of shared memory
 constexpr int kPassSmemBytes = (1 << kLogTile) * 32;
 
 cudaError_t launch_ntt_pass(int field, const PassParams& pp, uint64_t num_tiles, cudaStream_t st);

@@ -776,7 +776,7 @@ int zntt_probe_imad(double* per_second) {
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  *per_second = (double)blocks * threads * iters * 32.0 / (ms * 1e-3);
+  *per_second = (double)blocks * threads * iters * 8.0 / (ms * 1e-3);
   return ZNTT_OK;
 }
 
