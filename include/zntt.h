@@ -122,6 +122,19 @@ enum zntt_mode {
 int zntt_ntt_device(const zntt_twiddles* tw, const uint64_t* d_src, uint64_t* d_dst, uint64_t* d_scratch,
                     int mode, void* stream);
 
+/* In-place transform of the 2^log_n device elements at d_data (log_n of the
+ * twiddle handle, at most 18) that allocates no memory.  No counterpart in the
+ * reference.  For callers that must not allocate device memory when they
+ * transform: services that reserve all device memory up front under a fixed
+ * budget, programs whose memory belongs to another allocator, and
+ * latency-critical paths where cudaMalloc/cudaFree would block.  Its scratch
+ * is an 8 MiB array inside the library, held by every device that loads the
+ * library until the process exits.  The first call on a device looks up that
+ * array's device address (make it before any stream capture).  All calls
+ * share the array: calls that overlap on the GPU race.  Larger transforms are
+ * rejected with ZNTT_ERR_INVALID_ARGUMENT. */
+int zntt_ntt_device_inplace_noalloc(const zntt_twiddles* tw, uint64_t* d_data, int mode, void* stream);
+
 /* Seeded uniform elements on the device: element i is the i-th
  * randomFieldElement draw (libs/rng/src/rng.zig:32-65) from the ChaCha20
  * stream keyed by seed32 with a zero nonce and counter from 0

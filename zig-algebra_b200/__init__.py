@@ -150,6 +150,7 @@ def lib():
         L.zntt_probe_imad.argtypes = [ctypes.POINTER(ctypes.c_double)]
         L.zntt_probe_modmul.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
         L.zntt_probe_mul_wide.argtypes = [ctypes.POINTER(ctypes.c_double)]
+        L.zntt_ntt_device_inplace_noalloc.argtypes = [vp, vp, i, vp]
         _lib = L
     return _lib
 
@@ -325,6 +326,16 @@ def ntt_device(tw: DeviceTwiddles, d_src: int, d_dst: int, mode: int = FORWARD, 
                stream: int = 0) -> None:
     """Transforms 2^tw.log_n device elements (pointers as ints) on `stream`."""
     _check(lib().zntt_ntt_device(tw.handle, d_src, d_dst, d_scratch or None, mode, stream or None))
+
+
+def ntt_device_inplace_noalloc(tw: DeviceTwiddles, d_data: int, mode: int = FORWARD, stream: int = 0) -> None:
+    """In-place transform of up to 2^18 device elements that allocates no memory.
+
+    For callers that must not allocate device memory while they transform
+    (a fixed up-front memory budget, memory owned by another allocator, or a
+    latency-critical path).  Its scratch is an 8 MiB array inside the library;
+    calls that overlap on the GPU share it and race."""
+    _check(lib().zntt_ntt_device_inplace_noalloc(tw.handle, d_data, mode, stream or None))
 
 
 def seed_bytes(seed: int) -> bytes:
