@@ -32,7 +32,9 @@ import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-PRODUCTS_PER_MODMUL = 136  # 32x32->64 products in one 8x32-bit CIOS field product (2*8*8 + 8)
+# Multiply-pipe issue slots per 8x32-bit CIOS field product: 2N^2 + N = 136
+# full 32x32->64 products, each two 32-bit IMAD slots (lo and hi).
+IMAD_PER_MODMUL = 272
 METRIC = "BN254-Fr NTT elems/s at 2^24"
 
 
@@ -72,7 +74,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
@@ -110,12 +112,12 @@ class ClockSampler:
 
 
 def read_traffic(log_n: int):
-    """DRAM bytes per pass launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", f"ntt_pass_bn254_fr_2p{log_n}.txt")
+    """DRAM bytes (read + write) per pass launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"ntt_pass_bn254_fr_2p{log_n}_dram.txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.startswith("dram_bytes_per_launch:"):
+        if line.startswith("dram_bytes_per_launch_mean:"):
             return float(line.split(":", 1)[1].split()[0])
     return None
 
@@ -278,8 +280,8 @@ def run_zntt(args, rank, world, local):
     z.freeTwiddles(F, htw)
 
     # Roofline: the pass kernel is the only kernel in the timed region.
-    wide = z.probe_mul_wide()
-    peak_modmul = wide / PRODUCTS_PER_MODMUL
+    imad = z.probe_imad()
+    peak_modmul = imad / IMAD_PER_MODMUL
     modmuls = n / 2 * log_n
     achieved = modmuls / (ms_step * 1e-3)
     peaks, peaks_kind = measured_peaks()
@@ -306,8 +308,8 @@ def run_zntt(args, rank, world, local):
         "gpu_launches": args.steps * passes,
         "roofline": {"bound": "imad", "achieved": achieved, "peak": peak_modmul, "unit": "modmul/s",
                      "frac": achieved / peak_modmul, "traffic": traffic,
-                     "peak_source": f"measured live: mad.wide.u32 probe {wide:.4g} products/s / "
-                                    f"{PRODUCTS_PER_MODMUL} products per 8x32-bit CIOS modmul",
+                     "peak_source": f"measured live: dependent mad.lo.u32 probe {imad:.4g} IMAD/s / "
+                                    f"{IMAD_PER_MODMUL} IMAD slots per 8x32-bit CIOS modmul",
                      "hbm": {"achieved": alg_bytes / (ms_step * 1e-3) / 1e9, "peak": peaks["hbm_gbs"],
                              "unit": "GB/s", "frac": alg_bytes / (ms_step * 1e-3) / 1e9 / peaks["hbm_gbs"],
                              "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peaks_kind})"}},
@@ -339,7 +341,7 @@ def cpu_baseline_sample(host_data, log_n):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="zntt", choices=["zntt", "reference"])
     ap.add_argument("--log-n", type=int, default=24)
