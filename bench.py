@@ -289,6 +289,11 @@ def run_zntt(args, rank, world, local):
     passes = __import__("math").ceil(log_n / 10) if log_n > 11 else 1
     traffic = read_traffic(log_n)
     tw.close()
+    extra = {}
+    if not args.headline_only:
+        with torch.cuda.stream(stream):
+            extra["batched"] = run_batched_config(z, torch, stream, steps=20, warmup=3)
+            extra["coset_lde"] = run_lde_config(z, torch, stream, steps=5, warmup=2)
     if pg:
         pg.barrier()
         pg.destroy_process_group()
@@ -315,12 +320,128 @@ def run_zntt(args, rank, world, local):
                              "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peaks_kind})"}},
         "clocks": clk,
     }
+    line.update(extra)
     if world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline_sample(orig, log_n)
         except Exception as e:  # noqa: BLE001 -- report, never fail the GPU line
             line["cpu_baseline"] = {"value": None, "error": str(e)}
     print(json.dumps(line), flush=True)
+
+
+class TableCache:
+    """Device twiddle tables per log n for one field."""
+
+    def __init__(self, z, F):
+        self.z, self.F, self.t = z, F, {}
+
+    def __call__(self, log_n):
+        if log_n not in self.t:
+            self.t[log_n] = self.z.DeviceTwiddles(self.F, log_n, self.z.primitiveRootOfUnity(self.F, log_n))
+        return self.t[log_n]
+
+    def close(self):
+        for t in self.t.values():
+            t.close()
+
+
+def time_region(torch, stream, fn, steps):
+    """CUDA-event time of `steps` calls of fn() on `stream`, in ms."""
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_batched_config(z, torch, stream, steps, warmup, seed=33):
+    """512 BN254-Fr transforms of 2^10..2^16 (log size uniform) plus 8 of 2^20,
+    directions 50/50 by seed: one persistent launch (CUDA graph) against one
+    plain launch sequence per polynomial; both must agree bit for bit."""
+    import numpy as np
+    F = z.BN254_FR
+    rng = np.random.default_rng(seed)
+    logs = [int(v) for v in rng.integers(10, 17, 512)] + [20] * 8
+    modes = [z.INVERSE if v < 0.5 else z.FORWARD for v in rng.random(len(logs))]
+    tabs = TableCache(z, F)
+    sptr = stream.cuda_stream
+    xs, ys, ps, jobs = [], [], [], []
+    for i, (L, m) in enumerate(zip(logs, modes)):
+        x = torch.empty((1 << L) * 4, dtype=torch.int64, device="cuda")
+        z.random_elements(F, seed * 100000 + i, x.data_ptr(), 1 << L, stream=sptr)
+        y, pl = torch.empty_like(x), torch.empty_like(x)
+        xs.append(x); ys.append(y); ps.append(pl)
+        jobs.append({"kind": z.JOB_NTT, "tw": tabs(L), "mode": m, "src": x.data_ptr(), "dst": y.data_ptr()})
+    elements = sum(1 << L for L in logs)
+    butterflies = sum((1 << L) // 2 * L for L in logs)
+
+    def plain():
+        for L, m, x, pl in zip(logs, modes, xs, ps):
+            z.ntt_device(tabs(L), x.data_ptr(), pl.data_ptr(), m, stream=sptr)
+
+    with z.Batch(F, jobs) as b:
+        info = b.info()
+        run = lambda: b.run(stream=sptr, graph=True)  # noqa: E731
+        for _ in range(warmup):
+            run()
+            plain()
+        ms_b = time_region(torch, stream, run, steps)
+        ms_p = time_region(torch, stream, plain, steps)
+        b.status()
+    exact = all(torch.equal(y, pl) for y, pl in zip(ys, ps))
+    tabs.close()
+    return {
+        "workload": "512 x 2^U{10..16} + 8 x 2^20 BN254-Fr, fwd/inv 50/50, one persistent launch (CUDA graph)",
+        "elements": elements, "jobs": len(logs), "items": info["items"], "grid": info["grid"],
+        "shape": info["shape"], "ms_per_batch": ms_b / steps, "value": elements * steps / (ms_b * 1e-3),
+        "plain_ms_per_batch": ms_p / steps, "plain_value": elements * steps / (ms_p * 1e-3),
+        "speedup_vs_plain": ms_p / ms_b, "modmul_per_s": butterflies * steps / (ms_b * 1e-3),
+        "unit": "elements/s", "bit_exact_vs_plain": exact,
+    }
+
+
+def run_lde_config(z, torch, stream, steps, warmup, seed=44):
+    """64 BLS12-381-Fr coset extensions 2^18 -> 2^20 (inverse, zero-pad, g^i with
+    g = 5, forward): one persistent launch against plain per-polynomial passes."""
+    F = z.BLS12_381_FR
+    shift = z.to_montgomery(F, 5)
+    tabs = TableCache(z, F)
+    sptr = stream.cuda_stream
+    evs, outs, pls, jobs = [], [], [], []
+    for i in range(64):
+        ev = torch.empty((1 << 18) * 4, dtype=torch.int64, device="cuda")
+        z.random_elements(F, seed * 1000 + i, ev.data_ptr(), 1 << 18, stream=sptr)
+        out = torch.empty((1 << 20) * 4, dtype=torch.int64, device="cuda")
+        pl = torch.empty_like(out)
+        evs.append(ev); outs.append(out); pls.append(pl)
+        jobs.append({"kind": z.JOB_COSET_LDE, "tw": tabs(20), "tw_in": tabs(18), "shift": shift,
+                     "src": ev.data_ptr(), "dst": out.data_ptr()})
+
+    def plain():
+        for ev, pl in zip(evs, pls):
+            z.coset_lde_device(tabs(18), tabs(20), shift, ev.data_ptr(), pl.data_ptr(), stream=sptr)
+
+    with z.Batch(F, jobs) as b:
+        run = lambda: b.run(stream=sptr, graph=True)  # noqa: E731
+        for _ in range(warmup):
+            run()
+            plain()
+        ms_b = time_region(torch, stream, run, steps)
+        ms_p = time_region(torch, stream, plain, steps)
+        b.status()
+    exact = all(torch.equal(o, p) for o, p in zip(outs, pls))
+    tabs.close()
+    modmuls = 64 * ((1 << 17) * 18 + (1 << 18) + (1 << 19) * 20)
+    return {
+        "workload": "64 x coset LDE 2^18 -> 2^20 BLS12-381-Fr (g = 5), one persistent launch (CUDA graph)",
+        "ms_per_batch": ms_b / steps, "value": 64 * (1 << 20) * steps / (ms_b * 1e-3), "unit": "output elements/s",
+        "plain_ms_per_batch": ms_p / steps, "speedup_vs_plain": ms_p / ms_b,
+        "modmul_per_s": modmuls * steps / (ms_b * 1e-3), "bit_exact_vs_plain": exact,
+    }
 
 
 def cpu_baseline_sample(host_data, log_n):
@@ -347,6 +468,7 @@ def main():
     ap.add_argument("--log-n", type=int, default=24)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true", help="skip the batched and coset-extension lines")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":

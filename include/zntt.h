@@ -135,6 +135,56 @@ int zntt_ntt_device(const zntt_twiddles* tw, const uint64_t* d_src, uint64_t* d_
  * rejected with ZNTT_ERR_INVALID_ARGUMENT. */
 int zntt_ntt_device_inplace_noalloc(const zntt_twiddles* tw, uint64_t* d_data, int mode, void* stream);
 
+/* ---- batches: many jobs in one persistent launch -----------------------------
+ * A batch plans every job into passes and every pass into tiles, queues the
+ * tiles level by level on the device, and runs them all in one persistent
+ * launch that drains the queue (each tile waits, bounded, for its job's
+ * previous pass).  Jobs of a batch share a field and may mix sizes and kinds. */
+enum zntt_job_kind {
+  ZNTT_JOB_NTT = 0,       /* nttWithTwiddles / inttWithTwiddles (libs/ntt/src/root.zig:148-212) */
+  ZNTT_JOB_COSET_LDE = 1  /* intt of 2^log_in evaluations, zero-pad, c_i *= g^i, ntt of 2^log_n:
+                             the composition of zig-ntt with libs/poly/src/vector.zig:24-32,68-73 */
+};
+typedef struct zntt_job {
+  int kind;                   /* zntt_job_kind */
+  int mode;                   /* NTT jobs: ZNTT_FORWARD or ZNTT_INVERSE */
+  const zntt_twiddles* tw;    /* the transform's table (coset extension: of the output size) */
+  const zntt_twiddles* tw_in; /* coset extension: table of the input size (its inverse mapping is used) */
+  const uint64_t* d_src;      /* 2^log_n device elements (coset extension: 2^log_in evaluations) */
+  uint64_t* d_dst;            /* 2^log_n device elements; NTT jobs may transform in place */
+  uint64_t shift[4];          /* coset extension: the shift g, Montgomery form */
+} zntt_job;
+typedef struct zntt_batch zntt_batch;
+
+/* Plans the jobs (shape: a pass shape index, or -1 for the tuned one) and
+ * uploads the work queue; buffers stay owned by the caller and must outlive
+ * the batch. */
+int zntt_batch_create(int field, const zntt_job* jobs, size_t n_jobs, int shape, zntt_batch** out);
+/* Resets the queue and launches the persistent kernel on `stream`. */
+int zntt_batch_run(zntt_batch* b, void* stream);
+/* The same, captured once into a CUDA graph and replayed on later calls. */
+int zntt_batch_run_graph(zntt_batch* b, void* stream);
+/* After the stream finished: ZNTT_OK, or ZNTT_ERR_TIMEOUT if a wait gave up. */
+int zntt_batch_status(zntt_batch* b);
+int zntt_batch_info(const zntt_batch* b, uint32_t* n_items, uint32_t* n_passes, int* grid, int* shape);
+int zntt_batch_destroy(zntt_batch* b);
+
+/* One coset low-degree extension with plain per-pass launches:
+ * d_out = ntt_{2^log_n}((intt_{2^log_in}(d_evals) zero-padded) . g^i), where
+ * log_in / log_n are those of tw_in / tw_out. */
+int zntt_coset_lde_device(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t shift[4],
+                          const uint64_t* d_evals, uint64_t* d_out, void* stream);
+
+/* ---- autotuner ------------------------------------------------------------------
+ * Times every pass shape and stage count per pass for each log n in
+ * [log_n_min, log_n_max] on this GPU and keeps the fastest; plans use the
+ * table from then on.  The table persists as JSON lines keyed by GPU name;
+ * zntt_init loads the file named by ZNTT_TUNE_FILE when it exists. */
+int zntt_autotune(int field, uint32_t log_n_min, uint32_t log_n_max);
+int zntt_tune_save(const char* path);
+int zntt_tune_load(const char* path);
+int zntt_tune_clear(void);
+
 /* Seeded uniform elements on the device: element i is the i-th
  * randomFieldElement draw (libs/rng/src/rng.zig:32-65) from the ChaCha20
  * stream keyed by seed32 with a zero nonce and counter from 0

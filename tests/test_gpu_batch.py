@@ -1,0 +1,186 @@
+"""Batches (one persistent launch over many jobs), coset low-degree extensions
+and the autotuner, checked bit-exactly against the plain per-job path and the
+oracle.  Needs a B200."""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+WORKERS = min(os.cpu_count() or 1, 64)
+
+
+@pytest.fixture(scope="module")
+def z(zntt):
+    zntt.init(0)
+    return zntt
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _vec(z, F, seed, n):
+    torch = _torch()
+    x = torch.empty(n * 4, dtype=torch.int64, device="cuda")
+    z.random_elements(F, seed, x.data_ptr(), n)
+    return x
+
+
+def _host(t):
+    return t.cpu().numpy().view(np.uint64).reshape(-1, 4).copy()
+
+
+class Tables:
+    """Device twiddle tables per log n, closed at the end."""
+
+    def __init__(self, z, F):
+        self.z, self.F, self.t = z, F, {}
+
+    def __call__(self, log_n):
+        if log_n not in self.t:
+            self.t[log_n] = self.z.DeviceTwiddles(self.F, log_n, self.z.primitiveRootOfUnity(self.F, log_n))
+        return self.t[log_n]
+
+    def close(self):
+        for t in self.t.values():
+            t.close()
+
+
+@pytest.mark.parametrize("shape", [-1, 0, 1])
+def test_mixed_batch_matches_per_job_launches(z, shape):
+    torch = _torch()
+    rng = np.random.default_rng(11)
+    for F in z.FIELDS:
+        tabs = Tables(z, F)
+        logs = [int(v) for v in rng.integers(1, 17, 40)] + [0, 11, 12, 20]
+        jobs, refs, outs = [], [], []
+        for i, L in enumerate(logs):
+            n = 1 << L
+            x = _vec(z, F, 500 + i, n)
+            mode = z.INVERSE if rng.random() < 0.5 else z.FORWARD
+            want = torch.empty_like(x)
+            z.ntt_device(tabs(L), x.data_ptr(), want.data_ptr(), mode)
+            if i % 3 == 0:  # in place
+                dst = x
+            else:
+                dst = torch.empty_like(x)
+            jobs.append({"kind": z.JOB_NTT, "tw": tabs(L), "mode": mode, "src": x.data_ptr(),
+                         "dst": dst.data_ptr()})
+            refs.append(want)
+            outs.append((x, dst))
+        torch.cuda.synchronize()
+        keep = [x.clone() for x, _ in outs]
+        with z.Batch(F, jobs, shape=shape) as b:
+            info = b.info()
+            assert info["items"] > 0 and info["passes"] >= len(jobs)
+            for rep, graph in enumerate([False, True, True]):
+                if rep:  # restore in-place inputs between replays
+                    for (x, dst), k in zip(outs, keep):
+                        x.copy_(k)
+                torch.cuda.synchronize()
+                b.run(graph=graph)
+                torch.cuda.synchronize()
+                b.status()
+                for i, ((x, dst), want) in enumerate(zip(outs, refs)):
+                    assert torch.equal(dst, want), f"{F} job {i} 2^{logs[i]} replay {rep}"
+        tabs.close()
+
+
+def test_coset_lde_matches_oracle_and_fixture(z):
+    torch = _torch()
+    c = json.load(open(os.path.join(GOLDEN, "coset_lde.json")))
+    F = z.BLS12_381_FR
+    fid = O.BLS12_381_FR
+    shift = O.from_int(fid, c["shift"])
+    tabs = Tables(z, F)
+    for log_in, blow in [(c["log_in"], c["log_blowup"]), (1, 2), (10, 2), (12, 1), (14, 2)]:
+        seed = c["seed"] if log_in == c["log_in"] else 900 + log_in
+        ev = _vec(z, F, seed, 1 << log_in)
+        out = torch.empty((1 << (log_in + blow)) * 4, dtype=torch.int64, device="cuda")
+        z.coset_lde_device(tabs(log_in), tabs(log_in + blow), shift, ev.data_ptr(), out.data_ptr())
+        torch.cuda.synchronize()
+        want = O.coset_lde(fid, _host(ev), log_in, blow, shift, workers=WORKERS)
+        np.testing.assert_array_equal(_host(out), want)
+        if log_in == c["log_in"]:
+            got = O.to_ints(O.from_mont(fid, _host(out)))
+            assert got == [int(v, 16) for v in c["output"]]
+    tabs.close()
+
+
+def test_coset_lde_full_size_against_oracle(z):
+    """One extension of the C4 size: 2^18 evaluations to 2^20 over BLS12-381-Fr."""
+    torch = _torch()
+    F, fid = z.BLS12_381_FR, O.BLS12_381_FR
+    shift = O.from_int(fid, 5)
+    tabs = Tables(z, F)
+    ev = _vec(z, F, 4040, 1 << 18)
+    out = torch.empty((1 << 20) * 4, dtype=torch.int64, device="cuda")
+    z.coset_lde_device(tabs(18), tabs(20), shift, ev.data_ptr(), out.data_ptr())
+    torch.cuda.synchronize()
+    want = O.coset_lde(fid, _host(ev), 18, 2, shift, workers=WORKERS)
+    np.testing.assert_array_equal(_host(out), want)
+    tabs.close()
+
+
+def test_batched_coset_extensions_and_mixed_kinds(z):
+    torch = _torch()
+    F, fid = z.BLS12_381_FR, O.BLS12_381_FR
+    shift = O.from_int(fid, 5)
+    tabs = Tables(z, F)
+    jobs, refs = [], []
+    for i, (li, lo) in enumerate([(10, 12), (12, 14), (8, 10), (13, 15), (6, 8)]):
+        ev = _vec(z, F, 70 + i, 1 << li)
+        out = torch.empty((1 << lo) * 4, dtype=torch.int64, device="cuda")
+        want = torch.empty_like(out)
+        z.coset_lde_device(tabs(li), tabs(lo), shift, ev.data_ptr(), want.data_ptr())
+        jobs.append({"kind": z.JOB_COSET_LDE, "tw": tabs(lo), "tw_in": tabs(li), "shift": shift,
+                     "src": ev.data_ptr(), "dst": out.data_ptr(), "_keep": (ev, out)})
+        refs.append((out, want))
+    for i, L in enumerate([9, 13, 16]):
+        x = _vec(z, F, 80 + i, 1 << L)
+        y = torch.empty_like(x)
+        want = torch.empty_like(x)
+        z.ntt_device(tabs(L), x.data_ptr(), want.data_ptr(), z.INVERSE)
+        jobs.append({"kind": z.JOB_NTT, "tw": tabs(L), "mode": z.INVERSE, "src": x.data_ptr(), "dst": y.data_ptr(),
+                     "_keep": (x, y)})
+        refs.append((y, want))
+    torch.cuda.synchronize()
+    with z.Batch(F, jobs) as b:
+        b.run(graph=True)
+        torch.cuda.synchronize()
+        b.status()
+    for i, (got, want) in enumerate(refs):
+        assert torch.equal(got, want), f"job {i}"
+    tabs.close()
+
+
+def test_autotune_persists_and_keeps_results(z, tmp_path):
+    torch = _torch()
+    F = z.BN254_FR
+    z.autotune(F, 10, 13)
+    path = str(tmp_path / "tune.json")
+    z.tune_save(path)
+    text = open(path).read()
+    assert '"log_n": 12' in text and '"kmax"' in text
+    z.tune_clear()
+    z.tune_load(path)
+    # transforms under the tuned plans still equal the oracle
+    for L in (10, 12, 13):
+        x = _vec(z, F, 3000 + L, 1 << L)
+        y = torch.empty_like(x)
+        root = z.primitiveRootOfUnity(F, L)
+        with z.DeviceTwiddles(F, L, root) as tw:
+            z.ntt_device(tw, x.data_ptr(), y.data_ptr(), z.FORWARD)
+        torch.cuda.synchronize()
+        want = _host(x)
+        O.ntt(O.BN254_FR, want, L, root)
+        np.testing.assert_array_equal(_host(y), want)
+    z.tune_clear()

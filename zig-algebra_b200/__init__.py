@@ -119,6 +119,16 @@ class _Stage(ctypes.Structure):
 
 _U64P = ctypes.POINTER(ctypes.c_uint64)
 _lib = None
+
+JOB_NTT = 0
+JOB_COSET_LDE = 1
+
+
+class Job(ctypes.Structure):
+    """zntt_job (include/zntt.h)."""
+    _fields_ = [("kind", ctypes.c_int), ("mode", ctypes.c_int), ("tw", ctypes.c_void_p),
+                ("tw_in", ctypes.c_void_p), ("d_src", ctypes.c_void_p), ("d_dst", ctypes.c_void_p),
+                ("shift", ctypes.c_uint64 * 4)]
 _device = None
 
 
@@ -151,6 +161,17 @@ def lib():
         L.zntt_probe_modmul.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
         L.zntt_probe_mul_wide.argtypes = [ctypes.POINTER(ctypes.c_double)]
         L.zntt_ntt_device_inplace_noalloc.argtypes = [vp, vp, i, vp]
+        L.zntt_batch_create.argtypes = [i, ctypes.POINTER(Job), sz, i, ctypes.POINTER(vp)]
+        L.zntt_batch_run.argtypes = [vp, vp]
+        L.zntt_batch_run_graph.argtypes = [vp, vp]
+        L.zntt_batch_status.argtypes = [vp]
+        L.zntt_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
+                                      ctypes.POINTER(i), ctypes.POINTER(i)]
+        L.zntt_batch_destroy.argtypes = [vp]
+        L.zntt_coset_lde_device.argtypes = [vp, vp, _U64P, vp, vp, vp]
+        L.zntt_autotune.argtypes = [i, ctypes.c_uint32, ctypes.c_uint32]
+        L.zntt_tune_save.argtypes = [ctypes.c_char_p]
+        L.zntt_tune_load.argtypes = [ctypes.c_char_p]
         _lib = L
     return _lib
 
@@ -210,6 +231,12 @@ def _p(a: np.ndarray):
 def _root(root) -> ctypes.Array:
     r = np.ascontiguousarray(np.asarray(root, dtype=np.uint64).reshape(4))
     return (ctypes.c_uint64 * 4)(*[int(v) for v in r])
+
+
+def to_montgomery(F: Field, x: int) -> np.ndarray:
+    """fromInt (libs/field/src/field.zig:911-921): x mod p in Montgomery limbs."""
+    v = (int(x) % F.modulus) * (1 << 256) % F.modulus
+    return np.array([(v >> (64 * k)) & 0xFFFFFFFFFFFFFFFF for k in range(4)], dtype=np.uint64)
 
 
 def primitiveRootOfUnity(F: Field, log_n: int) -> np.ndarray:
@@ -375,3 +402,80 @@ def probe_modmul(F: Field) -> float:
     v = ctypes.c_double()
     _check(lib().zntt_probe_modmul(F.id, ctypes.byref(v)))
     return v.value
+
+
+# --- batches, coset extensions, autotuner ----------------------------------------------------
+
+class Batch:
+    """Many jobs (transforms and coset extensions) run by one persistent launch.
+
+    `jobs` is a list of dicts: {"kind": JOB_NTT, "tw": DeviceTwiddles, "mode": FORWARD,
+    "src": ptr, "dst": ptr} or {"kind": JOB_COSET_LDE, "tw": out table, "tw_in": in table,
+    "shift": 4 Montgomery limbs, "src": ptr, "dst": ptr}.  Device buffers stay owned by the
+    caller and must outlive the batch."""
+
+    def __init__(self, F: Field, jobs, shape: int = -1):
+        _ensure_init()
+        arr = (Job * max(len(jobs), 1))()
+        for i, j in enumerate(jobs):
+            arr[i].kind = j.get("kind", JOB_NTT)
+            arr[i].mode = j.get("mode", FORWARD)
+            arr[i].tw = j["tw"].handle
+            arr[i].tw_in = j["tw_in"].handle if j.get("tw_in") is not None else None
+            arr[i].d_src = j["src"]
+            arr[i].d_dst = j["dst"]
+            if "shift" in j:
+                for k, v in enumerate(np.asarray(j["shift"], dtype=np.uint64).reshape(4)):
+                    arr[i].shift[k] = int(v)
+        h = ctypes.c_void_p()
+        _check(lib().zntt_batch_create(F.id, arr, len(jobs), shape, ctypes.byref(h)))
+        self.handle = h
+
+    def run(self, stream: int = 0, graph: bool = False) -> None:
+        fn = lib().zntt_batch_run_graph if graph else lib().zntt_batch_run
+        _check(fn(self.handle, stream or None))
+
+    def status(self) -> None:
+        _check(lib().zntt_batch_status(self.handle))
+
+    def info(self) -> dict:
+        ni, npp = ctypes.c_uint32(), ctypes.c_uint32()
+        g, sh = ctypes.c_int(), ctypes.c_int()
+        _check(lib().zntt_batch_info(self.handle, ctypes.byref(ni), ctypes.byref(npp), ctypes.byref(g),
+                                     ctypes.byref(sh)))
+        return {"items": ni.value, "passes": npp.value, "grid": g.value, "shape": sh.value}
+
+    def close(self) -> None:
+        if self.handle:
+            lib().zntt_batch_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def coset_lde_device(tw_in: DeviceTwiddles, tw_out: DeviceTwiddles, shift, d_evals: int, d_out: int,
+                     stream: int = 0) -> None:
+    """One coset low-degree extension with plain per-pass launches."""
+    _check(lib().zntt_coset_lde_device(tw_in.handle, tw_out.handle, _root(shift), d_evals, d_out, stream or None))
+
+
+def autotune(F: Field, log_n_min: int, log_n_max: int) -> None:
+    _ensure_init()
+    _check(lib().zntt_autotune(F.id, log_n_min, log_n_max))
+
+
+def tune_save(path: str) -> None:
+    _check(lib().zntt_tune_save(path.encode()))
+
+
+def tune_load(path: str) -> None:
+    _ensure_init()
+    _check(lib().zntt_tune_load(path.encode()))
+
+
+def tune_clear() -> None:
+    lib().zntt_tune_clear()

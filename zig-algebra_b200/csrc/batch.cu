@@ -1,0 +1,151 @@
+// batch.cu -- many transforms (and coset low-degree extensions) in one
+// persistent launch that drains a device work queue.
+//
+// A job is one zig-ntt transform (nttWithTwiddles / inttWithTwiddles
+// semantics, libs/ntt/src/root.zig:148-212) or one FRI-style coset extension
+// (inverse transform of 2^log_in evaluations, zero-pad to 2^log_n, scale
+// coefficient i by g^i, forward transform; the composition of zig-ntt and
+// libs/poly/src/vector.zig:24-32,68-73).  Each job is planned into passes;
+// each pass into tiles.  The queue lists every (pass, tile) item level by
+// level, so every item's prerequisite pass has a lower queue index: an item
+// only waits for tiles already taken by CTAs that are running, and the queue
+// cannot deadlock whatever the grid size.  Waits are bounded; on timeout the
+// kernel raises an error flag and every CTA stops at its next item.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "field.cuh"
+#include "pass_tile.cuh"
+#include "runtime.hpp"
+
+namespace zntt {
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+template <class F, int LOG_TILE, int THREADS, int MINB, bool EXT>
+__global__ void __launch_bounds__(THREADS, MINB)
+    batch_kernel(const BatchPass* __restrict__ passes, const BatchItem* __restrict__ items, uint32_t n_items,
+                 uint32_t* ctl, uint32_t spin_limit) {
+  extern __shared__ uint4 sm[];
+  __shared__ PassParams s_pp;
+  __shared__ uint32_t s_item, s_ok;
+  constexpr int kWords = sizeof(PassParams) / 4;
+  for (;;) {
+    __syncthreads();  // the previous tile's shared-memory reads are done
+    if (threadIdx.x == 0) {
+      uint32_t it = n_items, ok = 1;
+      if (ld_relaxed(&ctl[1]) == 0) it = atomicAdd(&ctl[0], 1u);
+      if (it < n_items) {
+        const uint32_t dep = passes[items[it].pass].dep;
+        if (dep != kNoDep) {
+          const uint32_t need = passes[dep].tiles;
+          uint32_t spins = 0;
+          while (ld_acquire(&ctl[2 + dep]) < need) {
+            if (ld_relaxed(&ctl[1]) != 0) {
+              ok = 0;
+              break;
+            }
+            if (++spins > spin_limit) {
+              atomicExch(&ctl[1], 1u);
+              ok = 0;
+              break;
+            }
+            __nanosleep(256);
+          }
+        }
+      }
+      s_item = it;
+      s_ok = ok;
+    }
+    __syncthreads();
+    const uint32_t it = s_item;
+    if (it >= n_items || !s_ok) break;
+    const BatchItem item = items[it];
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&passes[item.pass].pp);
+    for (int w = threadIdx.x; w < kWords; w += THREADS) reinterpret_cast<uint32_t*>(&s_pp)[w] = src[w];
+    __syncthreads();
+    ntt_tile<F, LOG_TILE, THREADS, true, EXT>(s_pp, item.tile, sm);
+    __threadfence();  // this thread's stores are visible device-wide ...
+    __syncthreads();  // ... for every thread of the CTA, before the count
+    if (threadIdx.x == 0) atomicAdd(&ctl[2 + item.pass], 1u);
+  }
+}
+
+template <class F, int SH, bool EXT>
+static void* batch_ptr() {
+  return (void*)batch_kernel<F, kShapes[SH].log_tile, kShapes[SH].threads, kShapes[SH].min_blocks, EXT>;
+}
+
+template <class F>
+static void* batch_kernel_ptr(int shape, bool ext) {
+  if (shape == 0) return ext ? batch_ptr<F, 0, true>() : batch_ptr<F, 0, false>();
+  return ext ? batch_ptr<F, 1, true>() : batch_ptr<F, 1, false>();
+}
+
+cudaError_t configure_batch_kernels() {
+  for (int sh = 0; sh < kNumShapes; sh++) {
+    for (int ext = 0; ext < 2; ext++) {
+      cudaError_t e = cudaFuncSetAttribute(batch_kernel_ptr<Bn254Fr>(sh, ext), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           shape_smem_bytes(sh));
+      if (e != cudaSuccess) return e;
+      e = cudaFuncSetAttribute(batch_kernel_ptr<Bls12381Fr>(sh, ext), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               shape_smem_bytes(sh));
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
+}
+
+int batch_grid(int field, int shape, bool ext) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  void* fn = field == kBn254Fr ? batch_kernel_ptr<Bn254Fr>(shape, ext) : batch_kernel_ptr<Bls12381Fr>(shape, ext);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kShapes[shape].threads, shape_smem_bytes(shape));
+  if (per_sm < 1) per_sm = 1;
+  return sms * per_sm;
+}
+
+template <class F, int SH, bool EXT>
+static void launch_batch_k(const BatchPass* passes, const BatchItem* items, uint32_t n_items, uint32_t* ctl,
+                           uint32_t spin_limit, int grid, cudaStream_t st) {
+  constexpr PassShape S = kShapes[SH];
+  batch_kernel<F, S.log_tile, S.threads, S.min_blocks, EXT>
+      <<<grid, S.threads, shape_smem_bytes(SH), st>>>(passes, items, n_items, ctl, spin_limit);
+}
+
+template <class F>
+static void launch_batch_typed(int shape, bool ext, const BatchPass* passes, const BatchItem* items, uint32_t n_items,
+                               uint32_t* ctl, uint32_t spin_limit, int grid, cudaStream_t st) {
+  if (shape == 0) {
+    if (ext) launch_batch_k<F, 0, true>(passes, items, n_items, ctl, spin_limit, grid, st);
+    else launch_batch_k<F, 0, false>(passes, items, n_items, ctl, spin_limit, grid, st);
+  } else {
+    if (ext) launch_batch_k<F, 1, true>(passes, items, n_items, ctl, spin_limit, grid, st);
+    else launch_batch_k<F, 1, false>(passes, items, n_items, ctl, spin_limit, grid, st);
+  }
+}
+
+cudaError_t launch_batch(int field, int shape, bool ext, const BatchPass* passes, const BatchItem* items,
+                         uint32_t n_items, uint32_t* ctl, uint32_t spin_limit, int grid, cudaStream_t st) {
+  if (field == kBn254Fr)
+    launch_batch_typed<Bn254Fr>(shape, ext, passes, items, n_items, ctl, spin_limit, grid, st);
+  else
+    launch_batch_typed<Bls12381Fr>(shape, ext, passes, items, n_items, ctl, spin_limit, grid, st);
+  return cudaGetLastError();
+}
+
+}  // namespace zntt

@@ -5,204 +5,64 @@
 // stages a tile of the vector in shared memory with coalesced 16-byte global
 // loads, runs several butterfly stages on it, and writes it back.  All
 // arithmetic is exact Montgomery arithmetic from field.cuh.
+#include <cstring>
+
 #include "field.cuh"
 #include "kernels.cuh"
+#include "pass_tile.cuh"
 
 namespace zntt {
 
-// Shared memory holds a tile as two planes of 16-byte halves: half h of tile
-// element e is at sm[h * kTileMax + e], so a warp touching 32 consecutive
-// elements reads 512 contiguous bytes per plane (no bank conflicts).
-constexpr uint32_t kTileMax = 1u << kLogTile;
-
-__device__ __forceinline__ fe sm_load(const uint4* sm, uint32_t e) {
-  uint4 lo = sm[e], hi = sm[kTileMax + e];
-  fe r;
-  r.v[0] = lo.x; r.v[1] = lo.y; r.v[2] = lo.z; r.v[3] = lo.w;
-  r.v[4] = hi.x; r.v[5] = hi.y; r.v[6] = hi.z; r.v[7] = hi.w;
-  return r;
-}
-__device__ __forceinline__ void sm_store(uint4* sm, uint32_t e, const fe& a) {
-  sm[e] = make_uint4(a.v[0], a.v[1], a.v[2], a.v[3]);
-  sm[kTileMax + e] = make_uint4(a.v[4], a.v[5], a.v[6], a.v[7]);
-}
-
-__device__ __forceinline__ uint32_t rev_bits(uint32_t x, uint32_t bits) {
-  return bits == 0 ? 0u : (__brev(x) >> (32 - bits));
-}
-
-// Twiddle of global stage s (1-based) for butterfly index jg, with the
-// forward (tw[s-1][jg]) or inttWithTwiddles (1 or -tw[s-1][2^(s-1) - jg])
-// mapping.  `stw` points at tw[s-1]; returns false when the factor is one
-// and the multiply can be skipped.
-template <class F>
-__device__ __forceinline__ bool twiddle(const PassParams& pp, const uint4* stw, uint64_t half_g, uint64_t jg,
-                                        fe& w) {
-  if (jg == 0 && (pp.inverse | pp.tw0_one)) return false;
-  if (!pp.inverse) {
-    w = fe_load_nc(stw + (jg << 1));
-  } else {
-    w = fe_neg<F>(fe_load_nc(stw + ((half_g - jg) << 1)));
-  }
-  return true;
-}
-
-// u, v -> u + w v, u - w v
-template <class F>
-__device__ __forceinline__ void butterfly(fe& u, fe& v, bool mul, const fe& w) {
-  const fe t = mul ? fe_mul<F>(w, v) : v;
-  v = fe_sub<F>(u, t);
-  u = fe_add<F>(u, t);
-}
-
-template <class F, int LOG_TILE, int THREADS, int MINB>
+template <class F, int LOG_TILE, int THREADS, int MINB, bool EXT>
 __global__ void __launch_bounds__(THREADS, MINB) ntt_pass_kernel(PassParams pp) {
-  constexpr uint32_t TILE_MAX = 1u << LOG_TILE;
   extern __shared__ uint4 sm[];
-  const uint32_t k = pp.k, c = pp.c, C = 1u << c;
-  const uint32_t tile = 1u << (k + c);
-  const uint32_t tid = threadIdx.x;
-  const uint64_t blk = blockIdx.x;
-
-  uint64_t hi_base = 0, m0 = 0, col0 = 0;
-  if (pp.first) {
-    col0 = blk << c;
-  } else {
-    const uint32_t mlog = pp.S - c;
-    hi_base = (blk >> mlog) << (pp.S + k);
-    m0 = (blk & ((1ull << mlog) - 1)) << c;
-  }
-  const uint32_t xcols_log = pp.log_n - k;
-
-  // ---- load: column-fastest, 16-byte halves ----
-#pragma unroll
-  for (uint32_t q = 0; q < 2 * TILE_MAX / THREADS; q++) {
-    const uint32_t idx = tid + q * THREADS;
-    if (idx < 2 * tile) {
-      const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
-      uint64_t g;
-      uint32_t t;
-      if (pp.first) {
-        g = ((uint64_t)row << xcols_log) + col0 + col;
-        t = rev_bits(row, k);
-      } else {
-        g = hi_base + ((uint64_t)row << pp.S) + m0 + col;
-        t = row;
-      }
-      sm[h * TILE_MAX + ((t << c) | col)] = pp.src[(g << 1) | h];
-    }
-  }
-  __syncthreads();
-
-  uint32_t i = 1;
-  // ---- an odd stage count starts with one radix-2 stage ----
-  if (k & 1) {
-    const uint64_t half_g = 1ull << pp.S;  // stage S+1
-    const uint4* stw = pp.tw + ((half_g - 1) << 1);
-#pragma unroll
-    for (uint32_t q = 0; q < TILE_MAX / 2 / THREADS; q++) {
-      const uint32_t b = tid + q * THREADS;
-      if (b < tile / 2) {
-        const uint32_t col = b & (C - 1), t0 = (b >> c) << 1;  // half = 1: j = 0
-        const uint64_t jg = pp.first ? 0 : m0 + col;
-        const uint32_t e0 = (t0 << c) | col, e1 = e0 + C;
-        fe u = sm_load(sm, e0), v = sm_load(sm, e1), w;
-        const bool mul = twiddle<F>(pp, stw, half_g, jg, w);
-        butterfly<F>(u, v, mul, w);
-        sm_store(sm, e0, u);
-        sm_store(sm, e1, v);
-      }
-    }
-    __syncthreads();
-    i = 2;
-  }
-
-  // ---- radix-4 groups: stages i and i+1 on four elements in registers ----
-  for (; i < k; i += 2) {
-    const uint32_t h = 1u << (i - 1);
-    const uint64_t half1 = 1ull << (pp.S + i - 1);  // stage S+i
-    const uint64_t half2 = half1 << 1;              // stage S+i+1
-    const uint4* stw1 = pp.tw + ((half1 - 1) << 1);
-    const uint4* stw2 = pp.tw + ((half2 - 1) << 1);
-#pragma unroll
-    for (uint32_t q = 0; q < TILE_MAX / 4 / THREADS; q++) {
-      const uint32_t ga = tid + q * THREADS;
-      if (ga < tile / 4) {
-        const uint32_t col = ga & (C - 1), g = ga >> c;
-        const uint32_t j = g & (h - 1);
-        const uint32_t t0 = ((g >> (i - 1)) << (i + 1)) | j;
-        const uint32_t e0 = (t0 << c) | col, eh = h << c;
-        uint64_t jg1, jg3;
-        if (pp.first) {
-          jg1 = j;
-          jg3 = j + h;
-        } else {
-          jg1 = ((uint64_t)j << pp.S) + m0 + col;
-          jg3 = jg1 + ((uint64_t)h << pp.S);
-        }
-        fe w1, w2, w3;
-        const bool m1 = twiddle<F>(pp, stw1, half1, jg1, w1);
-        const bool m2 = twiddle<F>(pp, stw2, half2, jg1, w2);
-        const bool m3 = twiddle<F>(pp, stw2, half2, jg3, w3);
-        fe x0 = sm_load(sm, e0), x1 = sm_load(sm, e0 + eh), x2 = sm_load(sm, e0 + 2 * eh),
-           x3 = sm_load(sm, e0 + 3 * eh);
-        butterfly<F>(x0, x1, m1, w1);
-        butterfly<F>(x2, x3, m1, w1);
-        butterfly<F>(x0, x2, m2, w2);
-        butterfly<F>(x1, x3, m3, w3);
-        sm_store(sm, e0, x0);
-        sm_store(sm, e0 + eh, x1);
-        sm_store(sm, e0 + 2 * eh, x2);
-        sm_store(sm, e0 + 3 * eh, x3);
-      }
-    }
-    __syncthreads();
-  }
-
-  if (pp.scale) {
-    fe sc;
-#pragma unroll
-    for (int q = 0; q < 8; q++) sc.v[q] = pp.scale_val[q];
-#pragma unroll
-    for (uint32_t q = 0; q < TILE_MAX / THREADS; q++) {
-      const uint32_t e = tid + q * THREADS;
-      if (e < tile) sm_store(sm, e, fe_mul<F>(sm_load(sm, e), sc));
-    }
-    __syncthreads();
-  }
-
-  // ---- store ----
-#pragma unroll
-  for (uint32_t q = 0; q < 2 * TILE_MAX / THREADS; q++) {
-    const uint32_t idx = tid + q * THREADS;
-    if (idx < 2 * tile) {
-      const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
-      uint64_t g;
-      if (pp.first) {
-        g = ((uint64_t)rev_bits((uint32_t)(col0 + col), xcols_log) << k) + row;
-      } else {
-        g = hi_base + ((uint64_t)row << pp.S) + m0 + col;
-      }
-      pp.dst[(g << 1) | h] = sm[h * TILE_MAX + ((row << c) | col)];
-    }
-  }
+  ntt_tile<F, LOG_TILE, THREADS, false, EXT>(pp, blockIdx.x, sm);
 }
 
-#define ZNTT_PASS(F) ntt_pass_kernel<F, kLogTile, kPassThreads, kPassMinBlocks>
+template <class F, int SH, bool EXT>
+static void* pass_ptr() {
+  return (void*)ntt_pass_kernel<F, kShapes[SH].log_tile, kShapes[SH].threads, kShapes[SH].min_blocks, EXT>;
+}
+
+template <class F>
+static cudaError_t set_pass_attrs() {
+  void* fns[4] = {pass_ptr<F, 0, false>(), pass_ptr<F, 0, true>(), pass_ptr<F, 1, false>(), pass_ptr<F, 1, true>()};
+  for (int i = 0; i < 4; i++) {
+    cudaError_t e = cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize, shape_smem_bytes(i / 2));
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
 
 cudaError_t configure_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(ZNTT_PASS(Bn254Fr), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       kPassSmemBytes);
+  cudaError_t e = set_pass_attrs<Bn254Fr>();
+  if (e == cudaSuccess) e = set_pass_attrs<Bls12381Fr>();
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(ZNTT_PASS(Bls12381Fr), cudaFuncAttributeMaxDynamicSharedMemorySize, kPassSmemBytes);
+  return configure_batch_kernels();
 }
 
-cudaError_t launch_ntt_pass(int field, const PassParams& pp, uint64_t num_tiles, cudaStream_t st) {
-  dim3 grid((unsigned)num_tiles);
-  if (field == kBn254Fr)
-    ZNTT_PASS(Bn254Fr)<<<grid, kPassThreads, kPassSmemBytes, st>>>(pp);
+template <class F, int SH>
+static void launch_pass_shape(bool ext, const PassParams& pp, dim3 grid, cudaStream_t st) {
+  constexpr PassShape S = kShapes[SH];
+  if (ext)
+    ntt_pass_kernel<F, S.log_tile, S.threads, S.min_blocks, true><<<grid, S.threads, shape_smem_bytes(SH), st>>>(pp);
   else
-    ZNTT_PASS(Bls12381Fr)<<<grid, kPassThreads, kPassSmemBytes, st>>>(pp);
+    ntt_pass_kernel<F, S.log_tile, S.threads, S.min_blocks, false><<<grid, S.threads, shape_smem_bytes(SH), st>>>(pp);
+}
+
+template <class F>
+static void launch_pass_typed(int shape, bool ext, const PassParams& pp, dim3 grid, cudaStream_t st) {
+  if (shape == 0) launch_pass_shape<F, 0>(ext, pp, grid, st);
+  else launch_pass_shape<F, 1>(ext, pp, grid, st);
+}
+
+cudaError_t launch_ntt_pass(int field, int shape, const PassParams& pp, uint64_t num_tiles, cudaStream_t st) {
+  dim3 grid((unsigned)num_tiles);
+  const bool ext = pass_needs_ext(pp);
+  if (field == kBn254Fr)
+    launch_pass_typed<Bn254Fr>(shape, ext, pp, grid, st);
+  else
+    launch_pass_typed<Bls12381Fr>(shape, ext, pp, grid, st);
   return cudaGetLastError();
 }
 
@@ -234,6 +94,33 @@ cudaError_t launch_twiddle_table(int field, const uint4* d_pw, uint4* d_table, u
     twiddle_table_kernel<Bn254Fr><<<(unsigned)blocks, 256, 0, st>>>(d_pw, d_table, log_n);
   else
     twiddle_table_kernel<Bls12381Fr><<<(unsigned)blocks, 256, 0, st>>>(d_pw, d_table, log_n);
+  return cudaGetLastError();
+}
+
+// out[i] = c * base^i from three host-made power tables of the base
+// (pw[0][i] = base^i, pw[1][i] = base^(1024 i), pw[2][i] = base^(2^20 i)).
+template <class F>
+__global__ void powers_kernel(const uint4* __restrict__ pw, fe c, uint4* __restrict__ out, uint64_t count) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t e0 = i & 1023, e1 = (i >> 10) & 1023, e2 = (uint32_t)(i >> 20);
+    fe r = fe_mul<F>(fe_load_nc(pw + 2 * e0), fe_load_nc(pw + 2 * (1024 + e1)));
+    r = fe_mul<F>(r, fe_load_nc(pw + 2 * (2048 + e2)));
+    fe_store(out + 2 * i, fe_mul<F>(r, c));
+  }
+}
+
+cudaError_t launch_powers(int field, const uint4* d_pw, const uint64_t* c, uint4* out, uint64_t count,
+                          cudaStream_t st) {
+  fe cv;
+  std::memcpy(cv.v, c, 32);
+  uint64_t blocks = (count + 255) / 256;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks == 0) return cudaSuccess;
+  if (field == kBn254Fr)
+    powers_kernel<Bn254Fr><<<(unsigned)blocks, 256, 0, st>>>(d_pw, cv, out, count);
+  else
+    powers_kernel<Bls12381Fr><<<(unsigned)blocks, 256, 0, st>>>(d_pw, cv, out, count);
   return cudaGetLastError();
 }
 

@@ -31,27 +31,54 @@ struct PassParams {
   uint32_t first;     // gather the input through the bit reversal
   uint32_t inverse;   // inttWithTwiddles mapping: w = 1 (j = 0) or -tw[s-1][2^(s-1) - j]
   uint32_t tw0_one;   // every stage's entry 0 is one (j = 0 needs no multiply)
-  uint32_t scale;     // multiply each output by scale_val after the last stage
+  uint32_t scale;     // multiply each output by scale_val (or scale_tab[q]) after the last stage
   uint32_t scale_val[8];
+  uint32_t src_log;   // first pass: natural input index >= 2^src_log reads as zero (zero padding)
+  const uint4* scale_tab;  // when non-null, output position q is scaled by scale_tab[q]
 };
 
-// Pass kernel shape (overridable at build time for tuning sweeps).
-#ifndef ZNTT_PASS_THREADS
-#define ZNTT_PASS_THREADS 256
-#endif
-#ifndef ZNTT_PASS_MIN_BLOCKS
-#define ZNTT_PASS_MIN_BLOCKS 3
-#endif
-#ifndef ZNTT_LOG_TILE
-#define ZNTT_LOG_TILE 11
-#endif
-constexpr int kPassThreads = ZNTT_PASS_THREADS;
-constexpr int kPassMinBlocks = ZNTT_PASS_MIN_BLOCKS;
-constexpr int kLogTile = ZNTT_LOG_TILE;                  // 2^11 elements = 64 KiB of shared memory
-constexpr int kPassSmemBytes = (1 << kLogTile) * 32;
+// Pass kernel shapes.  Each shape is a compiled kernel: a tile of 2^log_tile
+// elements (32 bytes each in shared memory), `threads` per CTA, `min_blocks`
+// CTAs per SM for the register budget.  The autotuner picks a shape and a
+// stage count per pass for each (field, log n).
+struct PassShape {
+  int log_tile, threads, min_blocks;
+};
+constexpr int kNumShapes = 2;
+constexpr PassShape kShapes[kNumShapes] = {{11, 256, 3}, {10, 256, 3}};
+constexpr int kLogTile = 11;  // the largest tile of any shape
+constexpr int kDefaultShape = 0;
 
-cudaError_t launch_ntt_pass(int field, const PassParams& pp, uint64_t num_tiles, cudaStream_t st);
+inline int shape_smem_bytes(int shape) { return (1 << kShapes[shape].log_tile) * 32; }
+
+// A pass that pads its input with zeros or scales by a table runs the
+// extension variant of the kernels.
+inline bool pass_needs_ext(const PassParams& pp) {
+  return (pp.first && pp.src_log < pp.log_n) || (pp.scale && pp.scale_tab != nullptr);
+}
+
+cudaError_t launch_ntt_pass(int field, int shape, const PassParams& pp, uint64_t num_tiles, cudaStream_t st);
 cudaError_t configure_kernels();
+cudaError_t configure_batch_kernels();
+
+// ---- batched persistent launch ----------------------------------------------
+// One pass of one job inside a batch, and one unit of work (a tile of a pass).
+struct BatchPass {
+  PassParams pp;
+  uint32_t tiles;  // tiles in this pass
+  uint32_t dep;    // pass that must finish first (kNoDep: none)
+};
+constexpr uint32_t kNoDep = 0xffffffffu;
+struct BatchItem {
+  uint32_t pass;
+  uint32_t tile;
+};
+// ctl[0]: next item, ctl[1]: error flag, ctl[2 + p]: finished tiles of pass p.
+// Every wait for a finished pass spins at most `spin_limit` rounds of ~1 us,
+// then raises the error flag; every CTA stops at the next item once it is set.
+cudaError_t launch_batch(int field, int shape, bool ext, const BatchPass* passes, const BatchItem* items,
+                         uint32_t n_items, uint32_t* ctl, uint32_t spin_limit, int grid, cudaStream_t st);
+int batch_grid(int field, int shape, bool ext);
 
 // Flat zig-ntt twiddle table for one (field, log_n, root): entry 2^s - 1 + j
 // of stage s is root^(j * 2^(log_n-1-s)).  The powers are assembled from three
@@ -59,6 +86,11 @@ cudaError_t configure_kernels();
 // pw[2][i] = root^(2^20 i), i < 1024 (each 1024 x 32 bytes, contiguous).
 cudaError_t launch_twiddle_table(int field, const uint4* d_pw, uint4* d_table, uint32_t log_n,
                                  cudaStream_t st);
+
+// out[i] = c * base^i for i < count (count <= 2^30), from the three power
+// tables of `base` laid out as for launch_twiddle_table.
+cudaError_t launch_powers(int field, const uint4* d_pw, const uint64_t* c, uint4* out, uint64_t count,
+                          cudaStream_t st);
 
 // dst[rev(i)] = src[i] for 2^log_n elements (out of place).
 cudaError_t launch_bit_reverse(const uint4* src, uint4* dst, uint32_t log_n, cudaStream_t st);

@@ -79,14 +79,15 @@ extern "C" int zntt_ntt_device_inplace_noalloc(const zntt_twiddles* tw, uint64_t
   // Pass plan in a fixed array (the planner's passes never exceed 4 here).
   PassDesc passes[8];
   uint32_t np = 0;
-  if (log_n <= (uint32_t)kLogTile) {
+  const uint32_t lt = kShapes[kDefaultShape].log_tile;
+  if (log_n <= lt) {
     passes[np++] = {0, log_n, 0};
   } else {
-    const uint32_t kmax = kLogTile - 1, P = (log_n + kmax - 1) / kmax;
+    const uint32_t kmax = lt - 1, P = (log_n + kmax - 1) / kmax;
     uint32_t S = 0;
     for (uint32_t p = 0; p < P && np < 8; p++) {
       const uint32_t k = log_n / P + (p < log_n % P ? 1 : 0);
-      uint32_t cc = kLogTile - k;
+      uint32_t cc = lt - k;
       const uint32_t lim = p == 0 ? log_n - k : S;
       if (cc > lim) cc = lim;
       passes[np++] = {S, k, cc};
@@ -122,8 +123,9 @@ extern "C" int zntt_ntt_device_inplace_noalloc(const zntt_twiddles* tw, uint64_t
     pp.tw0_one = e->tw0_one;
     pp.scale = last && inverse;
     if (pp.scale) std::memcpy(pp.scale_val, ninv, 32);
+    pp.src_log = log_n;
     const uint64_t tiles = (1ull << log_n) >> (pp.k + pp.c);
-    ce = launch_ntt_pass(e->field, pp, tiles, st);
+    ce = launch_ntt_pass(e->field, kDefaultShape, pp, tiles, st);
     if (ce != cudaSuccess) return cuda_fail(ce, "ntt pass launch");
   }
   return ZNTT_OK;

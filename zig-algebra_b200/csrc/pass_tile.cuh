@@ -1,0 +1,214 @@
+// pass_tile.cuh -- one tile of one fused DIT pass, shared by the plain pass
+// kernel and the batched persistent kernel.
+//
+// The network is zig-ntt's (libs/ntt/src/root.zig:148-212): stage s pairs
+// DIT positions q and q + 2^(s-1) inside blocks of 2^s with twiddle
+// tw[s-1][q mod 2^(s-1)].  A tile holds the 2^k positions that differ only in
+// bits [S, S+k) of q, times 2^c neighbouring low-bit positions, in shared
+// memory as two planes of 16-byte halves (half h of tile element e at
+// sm[h * TILE + e]); stages run two at a time on four elements in registers.
+#pragma once
+
+#include "field.cuh"
+#include "kernels.cuh"
+
+namespace zntt {
+
+__device__ __forceinline__ uint32_t rev_bits(uint32_t x, uint32_t bits) {
+  return bits == 0 ? 0u : (__brev(x) >> (32 - bits));
+}
+
+template <uint32_t TILE>
+__device__ __forceinline__ fe sm_load(const uint4* sm, uint32_t e) {
+  uint4 lo = sm[e], hi = sm[TILE + e];
+  fe r;
+  r.v[0] = lo.x; r.v[1] = lo.y; r.v[2] = lo.z; r.v[3] = lo.w;
+  r.v[4] = hi.x; r.v[5] = hi.y; r.v[6] = hi.z; r.v[7] = hi.w;
+  return r;
+}
+template <uint32_t TILE>
+__device__ __forceinline__ void sm_store(uint4* sm, uint32_t e, const fe& a) {
+  sm[e] = make_uint4(a.v[0], a.v[1], a.v[2], a.v[3]);
+  sm[TILE + e] = make_uint4(a.v[4], a.v[5], a.v[6], a.v[7]);
+}
+
+// Twiddle of global stage s (1-based) for butterfly index jg, with the
+// forward (tw[s-1][jg]) or inttWithTwiddles (1 or -tw[s-1][2^(s-1) - jg])
+// mapping.  `stw` points at tw[s-1]; returns false when the factor is one and
+// the multiply can be skipped.
+template <class F>
+__device__ __forceinline__ bool twiddle(const PassParams& pp, const uint4* stw, uint64_t half_g, uint64_t jg,
+                                        fe& w) {
+  if (jg == 0 && (pp.inverse | pp.tw0_one)) return false;
+  if (!pp.inverse) {
+    w = fe_load_nc(stw + (jg << 1));
+  } else {
+    w = fe_neg<F>(fe_load_nc(stw + ((half_g - jg) << 1)));
+  }
+  return true;
+}
+
+// u, v -> u + w v, u - w v
+template <class F>
+__device__ __forceinline__ void butterfly(fe& u, fe& v, bool mul, const fe& w) {
+  const fe t = mul ? fe_mul<F>(w, v) : v;
+  v = fe_sub<F>(u, t);
+  u = fe_add<F>(u, t);
+}
+
+// Global loads of tile data: COHERENT reads through L2 only, for data other
+// SMs wrote earlier in the same launch (the batched kernel).
+template <bool COHERENT>
+__device__ __forceinline__ uint4 load_data(const uint4* p) {
+  if constexpr (COHERENT) return __ldcg(p);
+  else return *p;
+}
+
+// EXT enables the coset-extension features: zero padding of the first pass's
+// input beyond 2^src_log and a per-position scale table.  Plain transforms
+// compile without them (fewer live registers in the hot loop).
+template <class F, int LOG_TILE, int THREADS, bool COHERENT, bool EXT>
+__device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uint4* sm) {
+  constexpr uint32_t TILE_MAX = 1u << LOG_TILE;
+  const uint32_t k = pp.k, c = pp.c, C = 1u << c;
+  const uint32_t tile = 1u << (k + c);
+  const uint32_t tid = threadIdx.x;
+
+  uint64_t hi_base = 0, m0 = 0, col0 = 0;
+  if (pp.first) {
+    col0 = blk << c;
+  } else {
+    const uint32_t mlog = pp.S - c;
+    hi_base = (blk >> mlog) << (pp.S + k);
+    m0 = (blk & ((1ull << mlog) - 1)) << c;
+  }
+  const uint32_t xcols_log = pp.log_n - k;
+  const uint64_t src_len = 1ull << pp.src_log;
+
+  // ---- load: column-fastest, 16-byte halves ----
+#pragma unroll
+  for (uint32_t q = 0; q < 2 * TILE_MAX / THREADS; q++) {
+    const uint32_t idx = tid + q * THREADS;
+    if (idx < 2 * tile) {
+      const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
+      uint64_t g;
+      uint32_t t;
+      uint4 val;
+      if (pp.first) {
+        g = ((uint64_t)row << xcols_log) + col0 + col;
+        t = rev_bits(row, k);
+        if (EXT && g >= src_len) val = make_uint4(0, 0, 0, 0);
+        else val = load_data<COHERENT>(pp.src + ((g << 1) | h));
+      } else {
+        g = hi_base + ((uint64_t)row << pp.S) + m0 + col;
+        t = row;
+        val = load_data<COHERENT>(pp.src + ((g << 1) | h));
+      }
+      sm[h * TILE_MAX + ((t << c) | col)] = val;
+    }
+  }
+  __syncthreads();
+
+  uint32_t i = 1;
+  // ---- an odd stage count starts with one radix-2 stage ----
+  if (k & 1) {
+    const uint64_t half_g = 1ull << pp.S;  // stage S+1
+    const uint4* stw = pp.tw + ((half_g - 1) << 1);
+#pragma unroll
+    for (uint32_t q = 0; q < TILE_MAX / 2 / THREADS; q++) {
+      const uint32_t b = tid + q * THREADS;
+      if (b < tile / 2) {
+        const uint32_t col = b & (C - 1), t0 = (b >> c) << 1;  // half = 1: j = 0
+        const uint64_t jg = pp.first ? 0 : m0 + col;
+        const uint32_t e0 = (t0 << c) | col, e1 = e0 + C;
+        fe u = sm_load<TILE_MAX>(sm, e0), v = sm_load<TILE_MAX>(sm, e1), w;
+        const bool mul = twiddle<F>(pp, stw, half_g, jg, w);
+        butterfly<F>(u, v, mul, w);
+        sm_store<TILE_MAX>(sm, e0, u);
+        sm_store<TILE_MAX>(sm, e1, v);
+      }
+    }
+    __syncthreads();
+    i = 2;
+  }
+
+  // ---- radix-4 groups: stages i and i+1 on four elements in registers ----
+  for (; i < k; i += 2) {
+    const uint32_t h = 1u << (i - 1);
+    const uint64_t half1 = 1ull << (pp.S + i - 1);  // stage S+i
+    const uint64_t half2 = half1 << 1;              // stage S+i+1
+    const uint4* stw1 = pp.tw + ((half1 - 1) << 1);
+    const uint4* stw2 = pp.tw + ((half2 - 1) << 1);
+#pragma unroll
+    for (uint32_t q = 0; q < TILE_MAX / 4 / THREADS; q++) {
+      const uint32_t ga = tid + q * THREADS;
+      if (ga < tile / 4) {
+        const uint32_t col = ga & (C - 1), g = ga >> c;
+        const uint32_t j = g & (h - 1);
+        const uint32_t t0 = ((g >> (i - 1)) << (i + 1)) | j;
+        const uint32_t e0 = (t0 << c) | col, eh = h << c;
+        uint64_t jg1, jg3;
+        if (pp.first) {
+          jg1 = j;
+          jg3 = j + h;
+        } else {
+          jg1 = ((uint64_t)j << pp.S) + m0 + col;
+          jg3 = jg1 + ((uint64_t)h << pp.S);
+        }
+        fe w1, w2, w3;
+        const bool m1 = twiddle<F>(pp, stw1, half1, jg1, w1);
+        const bool m2 = twiddle<F>(pp, stw2, half2, jg1, w2);
+        const bool m3 = twiddle<F>(pp, stw2, half2, jg3, w3);
+        fe x0 = sm_load<TILE_MAX>(sm, e0), x1 = sm_load<TILE_MAX>(sm, e0 + eh),
+           x2 = sm_load<TILE_MAX>(sm, e0 + 2 * eh), x3 = sm_load<TILE_MAX>(sm, e0 + 3 * eh);
+        butterfly<F>(x0, x1, m1, w1);
+        butterfly<F>(x2, x3, m1, w1);
+        butterfly<F>(x0, x2, m2, w2);
+        butterfly<F>(x1, x3, m3, w3);
+        sm_store<TILE_MAX>(sm, e0, x0);
+        sm_store<TILE_MAX>(sm, e0 + eh, x1);
+        sm_store<TILE_MAX>(sm, e0 + 2 * eh, x2);
+        sm_store<TILE_MAX>(sm, e0 + 3 * eh, x3);
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- the inverse's 1/n (or a per-position factor table), then store ----
+  if (pp.scale) {
+    fe sc;
+#pragma unroll
+    for (int q = 0; q < 8; q++) sc.v[q] = pp.scale_val[q];
+#pragma unroll
+    for (uint32_t q = 0; q < TILE_MAX / THREADS; q++) {
+      const uint32_t e = tid + q * THREADS;
+      if (e < tile) {
+        const uint32_t col = e & (C - 1), row = e >> c;
+        if (EXT && pp.scale_tab) {
+          const uint64_t g = pp.first ? ((uint64_t)rev_bits((uint32_t)(col0 + col), xcols_log) << k) + row
+                                      : hi_base + ((uint64_t)row << pp.S) + m0 + col;
+          sc = fe_load_nc(pp.scale_tab + (g << 1));
+        }
+        sm_store<TILE_MAX>(sm, e, fe_mul<F>(sm_load<TILE_MAX>(sm, e), sc));
+      }
+    }
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (uint32_t q = 0; q < 2 * TILE_MAX / THREADS; q++) {
+    const uint32_t idx = tid + q * THREADS;
+    if (idx < 2 * tile) {
+      const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
+      uint64_t g;
+      if (pp.first) {
+        g = ((uint64_t)rev_bits((uint32_t)(col0 + col), xcols_log) << k) + row;
+      } else {
+        g = hi_base + ((uint64_t)row << pp.S) + m0 + col;
+      }
+      pp.dst[(g << 1) | h] = sm[h * TILE_MAX + ((row << c) | col)];
+    }
+  }
+}
+
+}  // namespace zntt

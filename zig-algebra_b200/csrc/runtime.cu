@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -101,45 +102,61 @@ struct PoolBuf {
 // pass planning
 // ---------------------------------------------------------------------------
 
-// Up to kLogTile stages run in one pass on a single tile of 2^log_n <= 2^kLogTile
-// elements.  Longer transforms are split into P = ceil(log_n / (kLogTile - 1))
-// passes of near-equal stage counts; each tile keeps 2^kLogTile elements, the
+// Up to log_tile stages run in one pass on a single tile of 2^log_n <=
+// 2^log_tile elements.  Longer transforms are split into P = ceil(log_n / kmax)
+// passes of near-equal stage counts; each tile keeps 2^log_tile elements, the
 // spare bits becoming 2^c contiguous positions per tile row.
-std::vector<PassDesc> plan_passes(uint32_t log_n) {
-  std::vector<PassDesc> out;
-  if (log_n == 0) return out;
-  if (log_n <= (uint32_t)kLogTile) {
-    out.push_back({0, log_n, 0});
-    return out;
+Plan make_plan(uint32_t log_n, int shape, uint32_t kmax) {
+  Plan plan;
+  plan.shape = shape;
+  const uint32_t lt = kShapes[shape].log_tile;
+  if (kmax < 2) kmax = 2;
+  if (kmax > lt) kmax = lt;
+  if (log_n == 0) return plan;
+  if (log_n <= lt) {
+    plan.p[plan.np++] = {0, log_n, 0};
+    return plan;
   }
-  const uint32_t kmax = kLogTile - 1;
   const uint32_t P = (log_n + kmax - 1) / kmax;
   uint32_t S = 0;
-  for (uint32_t p = 0; p < P; p++) {
-    uint32_t k = log_n / P + (p < log_n % P ? 1 : 0);
-    uint32_t c = kLogTile - k;
-    uint32_t lim = p == 0 ? log_n - k : S;  // columns available to a tile
+  for (uint32_t p = 0; p < P && plan.np < 8; p++) {
+    const uint32_t k = log_n / P + (p < log_n % P ? 1 : 0);
+    uint32_t c = lt - k;
+    const uint32_t lim = p == 0 ? log_n - k : S;  // columns available to a tile
     if (c > lim) c = lim;
-    out.push_back({S, k, c});
+    plan.p[plan.np++] = {S, k, c};
     S += k;
   }
-  return out;
+  return plan;
 }
 
-int run_transform(int field, const TwEntry* tw, uint32_t log_n, const uint4* d_src, uint4* d_dst, uint4* d_scratch,
-                  bool inverse, bool scale, const uint64_t* scale_val, cudaStream_t st) {
+uint32_t tuned_kmax(int field, uint32_t log_n, int shape) {
+  for (const TuneEntry& t : ctx().tune)
+    if (t.field == field && t.log_n == log_n && t.shape == shape) return t.kmax;
+  return kShapes[shape].log_tile - 1;
+}
+
+Plan tuned_plan(int field, uint32_t log_n) {
+  const TuneEntry* best = nullptr;
+  for (const TuneEntry& t : ctx().tune)
+    if (t.field == field && t.log_n == log_n && (!best || t.us < best->us)) best = &t;
+  if (best) return make_plan(log_n, best->shape, best->kmax);
+  return make_plan(log_n, kDefaultShape, kShapes[kDefaultShape].log_tile - 1);
+}
+
+int run_plan(int field, const TwEntry* tw, const Plan& plan, uint32_t log_n, const uint4* d_src, uint4* d_dst,
+             uint4* d_scratch, bool inverse, bool scale, const uint64_t* scale_val, cudaStream_t st) {
   if (log_n == 0) {
     // A length-1 transform has no stages; the inverse scale is by 1/1 = 1.
     if (d_src != d_dst) ZCHECK(cudaMemcpyAsync(d_dst, d_src, 32, cudaMemcpyDeviceToDevice, st), "copy");
     return ZNTT_OK;
   }
-  auto passes = plan_passes(log_n);
   const uint4* cur_src = d_src;
-  uint4* mid = (passes.size() == 1) ? d_dst : (d_dst != d_src ? d_dst : d_scratch);
+  uint4* mid = (plan.np == 1) ? d_dst : (d_dst != d_src ? d_dst : d_scratch);
   if (!mid) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "in-place multi-pass transform needs scratch");
-  for (size_t p = 0; p < passes.size(); p++) {
-    const PassDesc& d = passes[p];
-    const bool last = p + 1 == passes.size();
+  for (uint32_t p = 0; p < plan.np; p++) {
+    const PassDesc& d = plan.p[p];
+    const bool last = p + 1 == plan.np;
     PassParams pp;
     std::memset(&pp, 0, sizeof(pp));
     pp.src = cur_src;
@@ -154,12 +171,29 @@ int run_transform(int field, const TwEntry* tw, uint32_t log_n, const uint4* d_s
     pp.tw0_one = tw->tw0_one;
     pp.scale = last && scale;
     if (pp.scale) std::memcpy(pp.scale_val, scale_val, 32);
+    pp.src_log = log_n;
     const uint64_t tiles = (1ull << log_n) >> (d.k + d.c);
-    ZCHECK(launch_ntt_pass(field, pp, tiles, st), "ntt pass launch");
+    ZCHECK(launch_ntt_pass(field, plan.shape, pp, tiles, st), "ntt pass launch");
     cur_src = pp.dst;
   }
   return ZNTT_OK;
 }
+
+int run_transform(int field, const TwEntry* tw, uint32_t log_n, const uint4* d_src, uint4* d_dst, uint4* d_scratch,
+                  bool inverse, bool scale, const uint64_t* scale_val, cudaStream_t st) {
+  return run_plan(field, tw, tuned_plan(field, log_n), log_n, d_src, d_dst, d_scratch, inverse, scale, scale_val,
+                  st);
+}
+
+int pool_get(size_t bytes, void** out) {
+  cudaError_t e = ctx().pool.acquire(bytes, out);
+  if (e != cudaSuccess) {
+    *out = nullptr;
+    return cuda_fail(e, "device buffer");
+  }
+  return ZNTT_OK;
+}
+void pool_put(void* p, size_t bytes) { ctx().pool.release(p, bytes); }
 
 // ---------------------------------------------------------------------------
 // twiddle tables
@@ -205,13 +239,13 @@ static void evict_tables(size_t need) {
   }
 }
 
-static int fill_table(TwEntry* e, cudaStream_t st) {
-  const HostField& F = host_field(e->field);
-  if (e->log_n == 0) return ZNTT_OK;
-  // pw[0][i] = root^i, pw[1][i] = root^(1024 i), pw[2][i] = root^(2^20 i), i < 1024.
-  std::vector<uint64_t> pw(3 * 1024 * 4);
+// pw[0][i] = base^i, pw[1][i] = base^(1024 i), pw[2][i] = base^(2^20 i), i < 1024:
+// the three tables the twiddle and powers kernels multiply together.
+void host_power_tables(int field, const uint64_t* base, std::vector<uint64_t>& pw) {
+  const HostField& F = host_field(field);
+  pw.assign(3 * 1024 * 4, 0);
   uint64_t step[4];
-  std::memcpy(step, e->root, 32);
+  std::memcpy(step, base, 32);
   for (int t = 0; t < 3; t++) {
     uint64_t cur[4];
     std::memcpy(cur, F.one, 32);
@@ -219,11 +253,16 @@ static int fill_table(TwEntry* e, cudaStream_t st) {
       std::memcpy(&pw[(t * 1024 + i) * 4], cur, 32);
       F.mul(cur, step, cur);
     }
-    // step^1024 for the next level
     uint64_t nxt[4];
     F.pow_u64(step, 1024, nxt);
     std::memcpy(step, nxt, 32);
   }
+}
+
+static int fill_table(TwEntry* e, cudaStream_t st) {
+  if (e->log_n == 0) return ZNTT_OK;
+  std::vector<uint64_t> pw;
+  host_power_tables(e->field, e->root, pw);
   PoolBuf d_pw;
   int rc = d_pw.get(pw.size() * 8);
   if (rc) return rc;
@@ -379,7 +418,7 @@ static int check_fits(size_t log_n) {
   return ZNTT_OK;
 }
 
-static void n_inverse(int field, uint32_t log_n, uint64_t* out) {
+void n_inverse(int field, uint32_t log_n, uint64_t* out) {
   const HostField& F = host_field(field);
   uint64_t nf[4];
   F.from_u64((uint64_t)1 << log_n, nf);
@@ -488,6 +527,11 @@ int zntt_init(int device) {
   ZCHECK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), "cudaStreamCreate");
   ZCHECK(configure_kernels(), "kernel attributes");
   c.device = device;
+  c.gpu_name = prop.name;
+  if (const char* tf = std::getenv("ZNTT_TUNE_FILE")) {
+    zntt_tune_load(tf);  // a missing or foreign file leaves the default plans
+    clear_error();
+  }
   return ZNTT_OK;
 }
 
@@ -718,7 +762,7 @@ int zntt_ntt_device(const zntt_twiddles* tw, const uint64_t* d_src, uint64_t* d_
   const bool inverse = mode == ZNTT_INVERSE;
   uint64_t ninv[4];
   if (inverse) n_inverse(e->field, e->log_n, ninv);
-  const bool need_scratch = d_src == d_dst && plan_passes(e->log_n).size() > 1;
+  const bool need_scratch = d_src == d_dst && tuned_plan(e->field, e->log_n).np > 1;
   if (need_scratch && !d_scratch) {
     // Borrow a pool buffer; it returns to the pool only after the stream has
     // finished with it, so wait here.

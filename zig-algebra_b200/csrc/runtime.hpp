@@ -42,7 +42,27 @@ struct Registration {
 struct PassDesc {
   uint32_t S, k, c;
 };
-std::vector<PassDesc> plan_passes(uint32_t log_n);
+struct Plan {
+  int shape = kDefaultShape;
+  uint32_t np = 0;
+  PassDesc p[8];
+};
+// Splits log_n stages into passes of at most kmax stages on tiles of the shape.
+Plan make_plan(uint32_t log_n, int shape, uint32_t kmax);
+// The plan the tuning table holds for (field, log_n), else the default shape
+// with kmax = log_tile - 1.
+Plan tuned_plan(int field, uint32_t log_n);
+// The tuned stage count for a given shape.
+uint32_t tuned_kmax(int field, uint32_t log_n, int shape);
+
+// One measured configuration of the autotuner.
+struct TuneEntry {
+  int field = 0;
+  uint32_t log_n = 0;
+  int shape = 0;
+  uint32_t kmax = 0;
+  double us = 0;
+};
 
 // Caching device allocator: freed buffers are kept by exact size for reuse.
 class BufferPool {
@@ -67,6 +87,8 @@ struct Context {
   BufferPool pool;
   uint64_t clock = 0;
   size_t table_cache_budget = (size_t)16 << 30;  // unreferenced root tables kept up to this
+  std::string gpu_name;
+  std::vector<TuneEntry> tune;  // best kmax per (field, log_n, shape) on this GPU
 };
 
 Context& ctx();
@@ -84,5 +106,16 @@ void release_table(TwEntry* e);
 // multiplies every output by `scale_val` (Montgomery form) after the last stage.
 int run_transform(int field, const TwEntry* tw, uint32_t log_n, const uint4* d_src, uint4* d_dst,
                   uint4* d_scratch, bool inverse, bool scale, const uint64_t* scale_val, cudaStream_t st);
+// The same with an explicit plan (used by the autotuner).
+int run_plan(int field, const TwEntry* tw, const Plan& plan, uint32_t log_n, const uint4* d_src, uint4* d_dst,
+             uint4* d_scratch, bool inverse, bool scale, const uint64_t* scale_val, cudaStream_t st);
+
+// Pool buffer helpers shared by the translation units.
+int pool_get(size_t bytes, void** out);
+void pool_put(void* p, size_t bytes);
+// n^-1 in Montgomery form.
+void n_inverse(int field, uint32_t log_n, uint64_t* out);
+// The three power tables of `base` the twiddle and powers kernels expand.
+void host_power_tables(int field, const uint64_t* base, std::vector<uint64_t>& pw);
 
 }  // namespace zntt
