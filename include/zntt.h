@@ -175,6 +175,61 @@ int zntt_batch_destroy(zntt_batch* b);
 int zntt_coset_lde_device(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t shift[4],
                           const uint64_t* d_evals, uint64_t* d_out, void* stream);
 
+/* ---- serving: a continuously batching request server ---------------------------
+ * Requests carry pinned host buffers.  A worker thread admits them in FIFO
+ * order while their device buffers fit the HBM budget, turns whatever is
+ * admitted into one batch (one persistent launch) whenever one of `slots`
+ * streams is free -- so new arrivals overlap on the device with batches
+ * already running -- and posts completions with CLOCK_MONOTONIC timestamps.
+ * Twiddle tables of every size served stay resident; device buffers return to
+ * the pool after each request and are reused.  `serial` runs one request at
+ * a time with plain per-pass launches (the baseline batching is measured
+ * against). */
+typedef struct zntt_server_config {
+  int field;
+  size_t hbm_budget_bytes;  /* device bytes for request buffers (inputs, outputs, scratch) */
+  int slots;                /* batches in flight at once (streams) */
+  int max_batch_jobs;       /* requests per batch */
+  uint32_t max_items;       /* tiles per batch queue */
+  int serial;               /* 1: one request at a time, plain launches */
+  size_t max_batch_bytes;   /* a batch stops growing past this many input+output bytes
+                               (0: 64 MiB); a larger request runs alone */
+} zntt_server_config;
+typedef struct zntt_request {
+  int kind;                 /* ZNTT_JOB_NTT or ZNTT_JOB_COSET_LDE */
+  int mode;                 /* NTT: ZNTT_FORWARD or ZNTT_INVERSE */
+  uint32_t log_n;           /* transform size; coset extension: output size */
+  uint32_t log_in;          /* coset extension: input size */
+  const uint64_t* h_in;     /* pinned host input (2^log_n, or 2^log_in evaluations) */
+  uint64_t* h_out;          /* pinned host output, 2^log_n elements */
+  uint64_t shift[4];        /* coset extension: g, Montgomery form */
+  uint64_t user_tag;
+  uint64_t arrival_ns;      /* CLOCK_MONOTONIC arrival time, for latency */
+} zntt_request;
+typedef struct zntt_completion {
+  uint64_t user_tag;
+  int status;               /* ZNTT_OK or the failure */
+  uint64_t arrival_ns, admit_ns, done_ns;
+} zntt_completion;
+typedef struct zntt_server_stats {
+  uint64_t submitted, completed, rejected, batches, max_batch_jobs, max_inflight_jobs, peak_bytes, pending;
+  uint64_t max_launch_ns;   /* longest host time spent forming and enqueueing one batch */
+  uint64_t max_batch_ns;    /* longest enqueue-to-completion time of one batch */
+} zntt_server_stats;
+typedef struct zntt_server zntt_server;
+
+int zntt_server_create(const zntt_server_config* cfg, zntt_server** out);
+/* Queues a request (any thread, non-blocking); ZNTT_ERR_REJECTED if it can
+ * never fit the budget. */
+int zntt_server_submit(zntt_server* s, const zntt_request* r);
+/* Moves up to `cap` completions to `out`, waiting up to wait_ms for one. */
+int zntt_server_poll(zntt_server* s, zntt_completion* out, size_t cap, size_t* n, int wait_ms);
+int zntt_server_stats_get(zntt_server* s, zntt_server_stats* st);
+/* Finishes every queued request, then frees the server. */
+int zntt_server_destroy(zntt_server* s);
+/* CLOCK_MONOTONIC in nanoseconds (the clock of arrival_ns / done_ns). */
+uint64_t zntt_now_ns(void);
+
 /* ---- autotuner ------------------------------------------------------------------
  * Times every pass shape and stage count per pass for each log n in
  * [log_n_min, log_n_max] on this GPU and keeps the fastest; plans use the

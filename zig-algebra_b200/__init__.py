@@ -124,6 +124,33 @@ JOB_NTT = 0
 JOB_COSET_LDE = 1
 
 
+class ServerConfig(ctypes.Structure):
+    """zntt_server_config (include/zntt.h)."""
+    _fields_ = [("field", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_size_t), ("slots", ctypes.c_int),
+                ("max_batch_jobs", ctypes.c_int), ("max_items", ctypes.c_uint32), ("serial", ctypes.c_int),
+                ("max_batch_bytes", ctypes.c_size_t)]
+
+
+class Request(ctypes.Structure):
+    """zntt_request (include/zntt.h)."""
+    _fields_ = [("kind", ctypes.c_int), ("mode", ctypes.c_int), ("log_n", ctypes.c_uint32),
+                ("log_in", ctypes.c_uint32), ("h_in", ctypes.c_void_p), ("h_out", ctypes.c_void_p),
+                ("shift", ctypes.c_uint64 * 4), ("user_tag", ctypes.c_uint64), ("arrival_ns", ctypes.c_uint64)]
+
+
+class Completion(ctypes.Structure):
+    """zntt_completion (include/zntt.h)."""
+    _fields_ = [("user_tag", ctypes.c_uint64), ("status", ctypes.c_int), ("arrival_ns", ctypes.c_uint64),
+                ("admit_ns", ctypes.c_uint64), ("done_ns", ctypes.c_uint64)]
+
+
+class ServerStats(ctypes.Structure):
+    """zntt_server_stats (include/zntt.h)."""
+    _fields_ = [(k, ctypes.c_uint64) for k in ("submitted", "completed", "rejected", "batches", "max_batch_jobs",
+                                               "max_inflight_jobs", "peak_bytes", "pending", "max_launch_ns",
+                                               "max_batch_ns")]
+
+
 class Job(ctypes.Structure):
     """zntt_job (include/zntt.h)."""
     _fields_ = [("kind", ctypes.c_int), ("mode", ctypes.c_int), ("tw", ctypes.c_void_p),
@@ -172,6 +199,12 @@ def lib():
         L.zntt_autotune.argtypes = [i, ctypes.c_uint32, ctypes.c_uint32]
         L.zntt_tune_save.argtypes = [ctypes.c_char_p]
         L.zntt_tune_load.argtypes = [ctypes.c_char_p]
+        L.zntt_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+        L.zntt_server_submit.argtypes = [vp, ctypes.POINTER(Request)]
+        L.zntt_server_poll.argtypes = [vp, ctypes.POINTER(Completion), sz, ctypes.POINTER(sz), i]
+        L.zntt_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats)]
+        L.zntt_server_destroy.argtypes = [vp]
+        L.zntt_now_ns.restype = ctypes.c_uint64
         _lib = L
     return _lib
 
@@ -479,3 +512,44 @@ def tune_load(path: str) -> None:
 
 def tune_clear() -> None:
     lib().zntt_tune_clear()
+
+
+class Server:
+    """The continuously batching request server (zntt_server_*)."""
+
+    def __init__(self, F: Field, hbm_budget_bytes: int, slots: int = 4, max_batch_jobs: int = 256,
+                 max_items: int = 1 << 20, serial: bool = False, max_batch_bytes: int = 0):
+        _ensure_init()
+        cfg = ServerConfig(F.id, hbm_budget_bytes, slots, max_batch_jobs, max_items, int(serial), max_batch_bytes)
+        h = ctypes.c_void_p()
+        _check(lib().zntt_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.handle, self.field = h, F
+        self._buf = (Completion * 1024)()
+
+    def submit(self, req: Request) -> None:
+        _check(lib().zntt_server_submit(self.handle, ctypes.byref(req)))
+
+    def poll(self, wait_ms: int = 0):
+        n = ctypes.c_size_t()
+        _check(lib().zntt_server_poll(self.handle, self._buf, len(self._buf), ctypes.byref(n), wait_ms))
+        return [(c.user_tag, c.status, c.arrival_ns, c.admit_ns, c.done_ns) for c in self._buf[:n.value]]
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().zntt_server_stats_get(self.handle, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def close(self) -> None:
+        if self.handle:
+            lib().zntt_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def now_ns() -> int:
+    return int(lib().zntt_now_ns())

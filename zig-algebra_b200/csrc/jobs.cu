@@ -19,22 +19,14 @@
 #include <string>
 #include <vector>
 
+#include "jobs.hpp"
 #include "runtime.hpp"
 
 namespace zntt {
 
-// n^-1 * g^i for i < 2^log_in, cached per (field, log_in, g).
-struct CosetTab {
-  int field;
-  uint32_t log_in;
-  uint64_t shift[4];
-  uint4* d = nullptr;
-  size_t bytes = 0;
-  int refs = 0;
-};
 static std::vector<CosetTab*> g_coset_tabs;
 
-static int acquire_coset_tab(int field, uint32_t log_in, const uint64_t* shift, CosetTab** out, cudaStream_t st) {
+int acquire_coset_tab(int field, uint32_t log_in, const uint64_t* shift, CosetTab** out, cudaStream_t st) {
   for (CosetTab* t : g_coset_tabs) {
     if (t->field == field && t->log_in == log_in && std::memcmp(t->shift, shift, 32) == 0) {
       t->refs++;
@@ -78,21 +70,21 @@ static int acquire_coset_tab(int field, uint32_t log_in, const uint64_t* shift, 
   return ZNTT_OK;
 }
 
-static void release_coset_tab(CosetTab* t) {
+// Tables stay resident when their last user lets go (a cudaFree would
+// synchronise the device behind work in flight, and the next extension of the
+// same size would rebuild the table); zntt_shutdown frees them.
+void release_coset_tab(CosetTab* t) {
   if (!t) return;
-  if (--t->refs <= 0) {
-    cudaFree(t->d);
-    g_coset_tabs.erase(std::remove(g_coset_tabs.begin(), g_coset_tabs.end(), t), g_coset_tabs.end());
-    delete t;
-  }
+  if (t->refs > 0) t->refs--;
 }
 
-// The passes of one job, in order, with the buffers they run between.
-struct JobPlan {
-  std::vector<PassParams> passes;  // tiles = 2^log_n >> (k + c)
-  std::vector<uint64_t> tiles;
-  size_t work = 0;                 // elements x stages, for ordering
-};
+void free_coset_tabs() {
+  for (CosetTab* t : g_coset_tabs) {
+    if (t->d) cudaFree(t->d);
+    delete t;
+  }
+  g_coset_tabs.clear();
+}
 
 static PassParams pass_params(const TwEntry* tw, uint32_t log_n, const PassDesc& d, bool first, bool inverse,
                               const uint4* src, uint4* dst) {
@@ -114,7 +106,7 @@ static PassParams pass_params(const TwEntry* tw, uint32_t log_n, const PassDesc&
 
 // A batch plan: the tuned plan, and for a length-1 vector one pass of no stage
 // (a copy, scaled by 1/1 for the inverse) so that every job writes its output.
-static Plan batch_plan(int field, uint32_t log_n, int shape) {
+Plan batch_plan(int field, uint32_t log_n, int shape) {
   Plan plan = make_plan(log_n, shape, tuned_kmax(field, log_n, shape));
   if (log_n == 0) {
     plan.np = 1;
@@ -125,7 +117,7 @@ static Plan batch_plan(int field, uint32_t log_n, int shape) {
 
 // Appends the passes of one transform src -> dst (mid: where passes after the
 // first run in place).
-static void plan_transform(JobPlan& jp, const TwEntry* tw, const Plan& plan, uint32_t log_n, const uint4* src,
+void plan_transform(JobPlan& jp, const TwEntry* tw, const Plan& plan, uint32_t log_n, const uint4* src,
                            uint4* mid, uint4* dst, bool inverse, const uint64_t* scale_val, const uint4* scale_tab,
                            uint32_t src_log) {
   for (uint32_t p = 0; p < plan.np; p++) {

@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 
+#include "jobs.hpp"
 #include "runtime.hpp"
 
 namespace zntt {
@@ -542,6 +543,7 @@ int zntt_shutdown(void) {
   cudaSetDevice(c.device);
   cudaStreamSynchronize(c.stream);
   while (!c.all_tables.empty()) free_entry(c.all_tables.back());
+  free_coset_tabs();
   c.regs.clear();
   c.pool.trim();
   cudaStreamDestroy(c.stream);
