@@ -240,6 +240,13 @@ int zntt_tune_save(const char* path);
 int zntt_tune_load(const char* path);
 int zntt_tune_clear(void);
 
+/* Transforms `count` host vectors of 2^log_n elements (log_n of the table) in
+ * place, nttWithTwiddles / inttWithTwiddles semantics, overlapping each
+ * vector's host<->device copies with its neighbours' transforms (three
+ * streams, both copy engines).  Synchronous; pinned host memory gives full
+ * PCIe bandwidth. */
+int zntt_ntt_host_many(const zntt_twiddles* tw, uint64_t* const* h_data, size_t count, int mode);
+
 /* Seeded uniform elements on the device: element i is the i-th
  * randomFieldElement draw (libs/rng/src/rng.zig:32-65) from the ChaCha20
  * stream keyed by seed32 with a zero nonce and counter from 0

@@ -322,3 +322,33 @@ def test_full_size_properties(z, fname, log_n):
     pts = O.dft_points(fid, _to_host(x), root, ks, workers=WORKERS)
     Xh = _to_host(X)
     np.testing.assert_array_equal(Xh[ks], pts)
+
+
+@pytest.mark.parametrize("log_n", [3, 16, 20])
+def test_pipelined_host_vectors_match_single_calls(z, log_n):
+    torch = _torch()
+    for F, fid in _fields(z):
+        n = 1 << log_n
+        root = z.primitiveRootOfUnity(F, log_n)
+        tw_host = z.precomputeTwiddles(F, log_n, root)
+        bufs, wants = [], []
+        for i in range(5):
+            x = O.random_elements(fid, 700 + i, n) if log_n < 20 else None
+            if x is None:
+                d = torch.empty(n * 4, dtype=torch.int64, device="cuda")
+                z.random_elements(F, 700 + i, d.data_ptr(), n)
+                x = _to_host(d)
+            pinned = torch.empty(n * 4, dtype=torch.int64, pin_memory=True)
+            pinned.numpy().view(np.uint64)[:] = x.reshape(-1)
+            w = x.copy()
+            z.inttWithTwiddles(F, w, log_n, tw_host) if i % 2 else z.nttWithTwiddles(F, w, log_n, tw_host)
+            bufs.append(pinned)
+            wants.append(w)
+        with z.DeviceTwiddles(F, log_n, root) as tw:
+            fw = [b.data_ptr() for i, b in enumerate(bufs) if i % 2 == 0]
+            iv = [b.data_ptr() for i, b in enumerate(bufs) if i % 2 == 1]
+            z.ntt_host_many(tw, fw, z.FORWARD)
+            z.ntt_host_many(tw, iv, z.INVERSE)
+        for b, w in zip(bufs, wants):
+            np.testing.assert_array_equal(b.numpy().view(np.uint64).reshape(-1, 4), w)
+        z.freeTwiddles(F, tw_host)

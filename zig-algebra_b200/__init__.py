@@ -205,6 +205,7 @@ def lib():
         L.zntt_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats)]
         L.zntt_server_destroy.argtypes = [vp]
         L.zntt_now_ns.restype = ctypes.c_uint64
+        L.zntt_ntt_host_many.argtypes = [vp, ctypes.POINTER(vp), sz, i]
         _lib = L
     return _lib
 
@@ -396,6 +397,13 @@ def ntt_device_inplace_noalloc(tw: DeviceTwiddles, d_data: int, mode: int = FORW
     latency-critical path).  Its scratch is an 8 MiB array inside the library;
     calls that overlap on the GPU share it and race."""
     _check(lib().zntt_ntt_device_inplace_noalloc(tw.handle, d_data, mode, stream or None))
+
+
+def ntt_host_many(tw: DeviceTwiddles, host_ptrs, mode: int = FORWARD) -> None:
+    """Transforms host vectors (addresses of 2^tw.log_n-element buffers) in place,
+    pipelining each vector's copies with its neighbours' transforms."""
+    arr = (ctypes.c_void_p * max(len(host_ptrs), 1))(*host_ptrs)
+    _check(lib().zntt_ntt_host_many(tw.handle, arr, len(host_ptrs), mode))
 
 
 def seed_bytes(seed: int) -> bytes:

@@ -546,6 +546,11 @@ int zntt_shutdown(void) {
   free_coset_tabs();
   c.regs.clear();
   c.pool.trim();
+  for (cudaStream_t& p : c.pipe)
+    if (p) {
+      cudaStreamDestroy(p);
+      p = nullptr;
+    }
   cudaStreamDestroy(c.stream);
   c.stream = nullptr;
   c.device = -1;

@@ -88,6 +88,7 @@ struct Context {
   uint64_t clock = 0;
   size_t table_cache_budget = (size_t)16 << 30;  // unreferenced root tables kept up to this
   std::string gpu_name;
+  cudaStream_t pipe[3] = {nullptr, nullptr, nullptr};  // streams of the pipelined host API
   std::vector<TuneEntry> tune;  // best kmax per (field, log_n, shape) on this GPU
 };
 
