@@ -184,3 +184,35 @@ def test_autotune_persists_and_keeps_results(z, tmp_path):
         O.ntt(O.BN254_FR, want, L, root)
         np.testing.assert_array_equal(_host(y), want)
     z.tune_clear()
+
+
+@pytest.mark.parametrize("shape", [0, 1])
+def test_every_pass_shape_matches_oracle(z, tmp_path, shape):
+    """Plans forced to one pass shape (through a tuning file) stay bit-exact."""
+    torch = _torch()
+    name = torch.cuda.get_device_name(0)
+    path = tmp_path / "tune.json"
+    lt = 11 if shape == 0 else 10
+    lines = [f' {{"gpu": "{name}", "field": {f}, "log_n": {L}, "shape": {shape}, "kmax": {k}, "us": 1.0}}'
+             for f in (0, 1) for L in range(1, 23) for k in [lt - 1 if L % 2 else lt - 3]]
+    path.write_text("[\n" + ",\n".join(lines) + "\n]\n")
+    z.tune_clear()
+    z.tune_load(str(path))
+    try:
+        for F in z.FIELDS:
+            fid = F.id
+            for L in (5, 11, 12, 15, 18, 21):
+                root = z.primitiveRootOfUnity(F, L)
+                x = _vec(z, F, 8000 + L, 1 << L)
+                with z.DeviceTwiddles(F, L, root) as tw:
+                    for mode in (z.FORWARD, z.INVERSE):
+                        y = torch.empty_like(x)
+                        z.ntt_device(tw, x.data_ptr(), y.data_ptr(), mode)
+                        torch.cuda.synchronize()
+                        want = _host(x)
+                        st, otw = O.precompute_twiddles(fid, L, root)
+                        O.ntt_with_twiddles(fid, want, L, otw, inverse=mode == z.INVERSE, workers=WORKERS,
+                                            inplace4=True)
+                        np.testing.assert_array_equal(_host(y), want, err_msg=f"{F} 2^{L} mode {mode}")
+    finally:
+        z.tune_clear()
