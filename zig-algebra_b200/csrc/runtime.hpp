@@ -9,7 +9,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/zntt.h"
+#include "zntt.h"
 #include "host_field.hpp"
 #include "kernels.cuh"
 
