@@ -423,9 +423,14 @@ def run_batched_config(z, torch, stream, steps, warmup, seed=33):
     tabs = TableCache(z, F)
     sptr = stream.cuda_stream
     xs, ys, ps, jobs = [], [], [], []
+    # All inputs are consecutive slices of one seeded stream (one generator call).
+    total = sum(1 << L for L in logs)
+    pool = torch.empty(total * 4, dtype=torch.int64, device="cuda")
+    z.random_elements(F, seed, pool.data_ptr(), total, stream=sptr)
+    off = 0
     for i, (L, m) in enumerate(zip(logs, modes)):
-        x = torch.empty((1 << L) * 4, dtype=torch.int64, device="cuda")
-        z.random_elements(F, seed * 100000 + i, x.data_ptr(), 1 << L, stream=sptr)
+        x = pool[off * 4:(off + (1 << L)) * 4]
+        off += 1 << L
         y, pl = torch.empty_like(x), torch.empty_like(x)
         xs.append(x); ys.append(y); ps.append(pl)
         jobs.append({"kind": z.JOB_NTT, "tw": tabs(L), "mode": m, "src": x.data_ptr(), "dst": y.data_ptr()})
@@ -465,9 +470,10 @@ def run_lde_config(z, torch, stream, steps, warmup, seed=44):
     tabs = TableCache(z, F)
     sptr = stream.cuda_stream
     evs, outs, pls, jobs = [], [], [], []
+    pool = torch.empty(64 * (1 << 18) * 4, dtype=torch.int64, device="cuda")
+    z.random_elements(F, seed, pool.data_ptr(), 64 << 18, stream=sptr)
     for i in range(64):
-        ev = torch.empty((1 << 18) * 4, dtype=torch.int64, device="cuda")
-        z.random_elements(F, seed * 1000 + i, ev.data_ptr(), 1 << 18, stream=sptr)
+        ev = pool[i * (1 << 18) * 4:(i + 1) * (1 << 18) * 4]
         out = torch.empty((1 << 20) * 4, dtype=torch.int64, device="cuda")
         pl = torch.empty_like(out)
         evs.append(ev); outs.append(out); pls.append(pl)
@@ -561,6 +567,28 @@ def run_serve(args):  # noqa: C901
     print(json.dumps(line), flush=True)
 
 
+def run_single_config(args):
+    """One of the batched configurations alone (for profiling): its JSON line."""
+    import torch
+    z = load_package()
+    torch.cuda.set_device(0)
+    z.init(0)
+    load_tuning(z)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    with torch.cuda.stream(stream):
+        if args.workload == "batched":
+            r = run_batched_config(z, torch, stream, steps=args.steps, warmup=args.warmup)
+            metric = "batched BN254-Fr NTT elems/s (512 x 2^U{10..16} + 8 x 2^20)"
+        else:
+            r = run_lde_config(z, torch, stream, steps=args.steps, warmup=args.warmup)
+            metric = "batched coset LDE output elems/s (64 x 2^18 -> 2^20, BLS12-381-Fr)"
+    line = {"metric": metric, "value": r["value"], "unit": r["unit"], "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "data": "synthetic: seeded inputs",
+            "config": {"workload": r["workload"]}, "detail": r}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -571,7 +599,7 @@ def main():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true", help="skip the batched and coset-extension lines")
-    ap.add_argument("--workload", default="ntt", choices=["ntt", "serve"])
+    ap.add_argument("--workload", default="ntt", choices=["ntt", "serve", "batched", "lde"])
     ap.add_argument("--serve-requests", type=int, default=20000)
     ap.add_argument("--serve-sweep", type=float, nargs="*", default=[8000.0, 32000.0])
     ap.add_argument("--serve-sweep-requests", type=int, default=6000)
@@ -580,6 +608,10 @@ def main():
     if args.workload == "serve":
         if rank == 0:
             run_serve(args)
+        return
+    if args.workload in ("batched", "lde"):
+        if rank == 0:
+            run_single_config(args)
         return
     if args.impl == "reference":
         run_reference(args, rank)
