@@ -48,12 +48,28 @@ __device__ __forceinline__ bool twiddle(const PassParams& pp, const uint4* stw, 
   return true;
 }
 
-// u, v -> u + w v, u - w v
+// u, v -> u + w v, u - w v.  Lazy fields (4p < 2^256) keep u and v in
+// [0, 2p) between stages; the last stage of a pass reduces them to [0, p), so
+// every pass reads and writes canonical elements.
 template <class F>
 __device__ __forceinline__ void butterfly(fe& u, fe& v, bool mul, const fe& w) {
-  const fe t = mul ? fe_mul<F>(w, v) : v;
-  v = fe_sub<F>(u, t);
-  u = fe_add<F>(u, t);
+  if constexpr (F::kLazy) {
+    const fe t = mul ? fe_mul<F, false>(w, v) : v;
+    v = fe_sub2p<F>(u, t);
+    u = fe_add2p<F>(u, t);
+  } else {
+    const fe t = mul ? fe_mul<F>(w, v) : v;
+    v = fe_sub<F>(u, t);
+    u = fe_add<F>(u, t);
+  }
+}
+
+// [0, 2p) -> [0, p) after a pass's last stage (lazy fields only).
+template <class F>
+__device__ __forceinline__ void canonical(fe& x, bool last) {
+  if constexpr (F::kLazy) {
+    if (last) x = fe_reduce<F>(x);
+  }
 }
 
 // Global loads of tile data: COHERENT reads through L2 only, for data other
@@ -124,6 +140,8 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
         fe u = sm_load<TILE_MAX>(sm, e0), v = sm_load<TILE_MAX>(sm, e1), w;
         const bool mul = twiddle<F>(pp, stw, half_g, jg, w);
         butterfly<F>(u, v, mul, w);
+        canonical<F>(u, k == 1);
+        canonical<F>(v, k == 1);
         sm_store<TILE_MAX>(sm, e0, u);
         sm_store<TILE_MAX>(sm, e1, v);
       }
@@ -165,6 +183,11 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
         butterfly<F>(x2, x3, m1, w1);
         butterfly<F>(x0, x2, m2, w2);
         butterfly<F>(x1, x3, m3, w3);
+        const bool last = i + 2 >= k;
+        canonical<F>(x0, last);
+        canonical<F>(x1, last);
+        canonical<F>(x2, last);
+        canonical<F>(x3, last);
         sm_store<TILE_MAX>(sm, e0, x0);
         sm_store<TILE_MAX>(sm, e0 + eh, x1);
         sm_store<TILE_MAX>(sm, e0 + 2 * eh, x2);
