@@ -38,6 +38,18 @@ IMAD_PER_MODMUL = 272
 METRIC = "BN254-Fr NTT elems/s at 2^24"
 
 
+def metric_name(log_n: int) -> str:
+    """The headline metric's name for a transform of 2^log_n (2^24 by default)."""
+    return METRIC if log_n == 24 else f"BN254-Fr NTT elems/s at 2^{log_n}"
+
+
+def l2_note(n: int) -> str:
+    mib = n * 32 / 2**20
+    if mib * 2**20 > 126e6:
+        return f"inputs ({mib:g} MiB per vector) larger than L2; no flush"
+    return f"inputs ({mib:g} MiB per vector) fit in L2 (126 MB); no flush"
+
+
 def load_package():
     name = "zig_algebra_b200"
     if name in sys.modules:
@@ -211,7 +223,7 @@ def run_reference(args, rank):
     if log_n != args.log_n:
         sample += f" (2^{log_n} per step: 2^{args.log_n} steps would not fit the time budget)"
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric_name(args.log_n), "value": value, "unit": "elements/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u256-mod-r (BN254-Fr)",
         "data": "synthetic: seeded ChaCha20 randomFieldElement draws",
@@ -350,13 +362,13 @@ def run_zntt(args, rank, world, local):
     if rank != 0:
         return
     line = {
-        "metric": METRIC, "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
+        "metric": metric_name(log_n), "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u256-mod-r (BN254-Fr, 8x32-bit Montgomery)",
         "data": "synthetic: seeded ChaCha20 randomFieldElement draws generated on the device",
         "config": {"workload": f"bn254_fr_ntt_forward_2^{log_n}", "log_n": log_n, "field": "bn254_fr",
                    "direction": "forward", "twiddles": "precomputed, device-resident",
-                   "l2": "inputs (512 MiB per vector) larger than L2; no flush", "passes": passes,
+                   "l2": l2_note(n), "passes": passes,
                    "parallelism": f"replicas x{world} (independent vectors, no collective)",
                    "tuning": os.path.relpath(tuning, ROOT) if tuning.startswith(ROOT) else tuning},
         "e2e": {"value": e2e_value, "unit": "elements/s", "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 32,
