@@ -356,6 +356,8 @@ def run_zntt(args, rank, world, local):
         with torch.cuda.stream(stream):
             extra["batched"] = run_batched_config(z, torch, stream, steps=20, warmup=3)
             extra["coset_lde"] = run_lde_config(z, torch, stream, steps=5, warmup=2)
+            extra["poly_mul"] = run_poly_config(z, torch, stream, steps=5, warmup=2,
+                                                cpu_sample=not args.no_cpu_baseline)
     if pg:
         pg.barrier()
         pg.destroy_process_group()
@@ -515,6 +517,90 @@ def run_lde_config(z, torch, stream, steps, warmup, seed=44):
     }
 
 
+def run_poly_config(z, torch, stream, steps, warmup, seed=55, cpu_sample=True):
+    """Polynomial.mul (libs/poly/src/poly.zig:197-212) on the device: one BN254-Fr product of
+    two 2^23-coefficient polynomials (three 2^24-point transforms, the pointwise product fused
+    into the second), and 64 products of two 2^14-coefficient polynomials in one persistent
+    launch against plain per-product launches.  The CPU figure is the reference's schoolbook
+    loop (the oracle port) on a bounded sample, extrapolated by its O(n^2) count."""
+    F = z.BN254_FR
+    sptr = stream.cuda_stream
+    tabs = TableCache(z, F)
+    n = 1 << 23
+    a = torch.empty(n * 4, dtype=torch.int64, device="cuda")
+    b = torch.empty_like(a)
+    z.random_elements(F, seed, a.data_ptr(), n, stream=sptr)
+    z.random_elements(F, seed + 1, b.data_ptr(), n, stream=sptr)
+    out = torch.empty((2 * n - 1) * 4, dtype=torch.int64, device="cuda")
+    one = lambda: z.poly_mul_device(tabs(24), a.data_ptr(), n, b.data_ptr(), n, out.data_ptr(), stream=sptr)  # noqa: E731
+    for _ in range(warmup):
+        one()
+    ms_one = time_region(torch, stream, one, steps) / steps
+    N = 1 << 24
+    modmuls = 3 * (N // 2) * 24 + 2 * N  # three transforms, the pointwise product, n^-1
+
+    m, count = 1 << 14, 64
+    pa = torch.empty(count * m * 4, dtype=torch.int64, device="cuda")
+    pb = torch.empty_like(pa)
+    z.random_elements(F, seed + 2, pa.data_ptr(), count * m, stream=sptr)
+    z.random_elements(F, seed + 3, pb.data_ptr(), count * m, stream=sptr)
+    outs = [torch.empty((2 * m - 1) * 4, dtype=torch.int64, device="cuda") for _ in range(count)]
+    pls = [torch.empty_like(o) for o in outs]
+    ptr = lambda t, i: t.data_ptr() + i * m * 32  # noqa: E731
+    jobs = [{"kind": z.JOB_POLY_MUL, "tw": tabs(15), "src": ptr(pa, i), "len": m, "src2": ptr(pb, i), "len2": m,
+             "dst": outs[i].data_ptr()} for i in range(count)]
+
+    def plain():
+        for i in range(count):
+            z.poly_mul_device(tabs(15), ptr(pa, i), m, ptr(pb, i), m, pls[i].data_ptr(), stream=sptr)
+
+    with z.Batch(F, jobs) as bt:
+        run = lambda: bt.run(stream=sptr, graph=True)  # noqa: E731
+        for _ in range(warmup):
+            run()
+            plain()
+        ms_b = time_region(torch, stream, run, steps) / steps
+        ms_p = time_region(torch, stream, plain, steps) / steps
+        bt.status()
+    exact = all(torch.equal(o, q) for o, q in zip(outs, pls))
+    tabs.close()
+    r = {
+        "workload": "BN254-Fr product of two 2^23-coefficient polynomials (three 2^24-point transforms)",
+        "ms": ms_one, "value": (2 * n - 1) / (ms_one * 1e-3), "unit": "product coefficients/s",
+        "modmul_per_s": modmuls / (ms_one * 1e-3),
+        "batched": {"workload": "64 products of two 2^14-coefficient BN254-Fr polynomials (2^15 points), one "
+                                "persistent launch (CUDA graph)",
+                    "ms_per_batch": ms_b, "plain_ms_per_batch": ms_p, "speedup_vs_plain": ms_p / ms_b,
+                    "bit_exact_vs_plain": exact},
+    }
+    if cpu_sample:
+        r["cpu_schoolbook"] = cpu_schoolbook_sample(n)
+    return r
+
+
+def cpu_schoolbook_sample(n_full, log_sample=12):
+    """Polynomial.mul's double loop (the oracle port, all host cores) on two 2^log_sample-
+    coefficient polynomials; its product rate extrapolates the full size's n^2 products."""
+    workers = min(os.cpu_count() or 1, 64)
+    O, lib = cpu_oracle(native=True)
+    k = 1 << log_sample
+    a = O.random_elements(O.BN254_FR, 1, k)
+    b = O.random_elements(O.BN254_FR, 2, k)
+    out = O.elems(2 * k - 1)
+    deg = ctypes.c_int64(0)
+    best = None
+    for _ in range(3):
+        t0 = time.perf_counter()
+        st = lib.zo_poly_mul(O.BN254_FR, O._p(a), k, O._p(b), k, 2 * k - 2, O._p(out), ctypes.byref(deg), workers)
+        dt = time.perf_counter() - t0
+        assert st == 0
+        best = dt if best is None else min(best, dt)
+    rate = k * k / best
+    return {"sample": f"2^{log_sample} x 2^{log_sample} coefficients, schoolbook on {workers} threads (best of 3)",
+            "products_per_s": rate, "cores": workers, "kind": "port",
+            "extrapolated_ms_full": n_full * n_full / rate * 1e3}
+
+
 def cpu_baseline_sample(host_data, log_n):
     """The oracle port on all host cores, on the same input, for one full transform."""
     workers = min(os.cpu_count() or 1, 64)
@@ -592,6 +678,10 @@ def run_single_config(args):
         if args.workload == "batched":
             r = run_batched_config(z, torch, stream, steps=args.steps, warmup=args.warmup)
             metric = "batched BN254-Fr NTT elems/s (512 x 2^U{10..16} + 8 x 2^20)"
+        elif args.workload == "poly":
+            r = run_poly_config(z, torch, stream, steps=args.steps, warmup=args.warmup,
+                                cpu_sample=not args.no_cpu_baseline)
+            metric = "BN254-Fr polynomial product coefficients/s (2^23 x 2^23 coefficients)"
         else:
             r = run_lde_config(z, torch, stream, steps=args.steps, warmup=args.warmup)
             metric = "batched coset LDE output elems/s (64 x 2^18 -> 2^20, BLS12-381-Fr)"
@@ -610,8 +700,9 @@ def main():
     ap.add_argument("--log-n", type=int, default=24)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--headline-only", action="store_true", help="skip the batched and coset-extension lines")
-    ap.add_argument("--workload", default="ntt", choices=["ntt", "serve", "batched", "lde"])
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the batched, coset-extension and polynomial-product lines")
+    ap.add_argument("--workload", default="ntt", choices=["ntt", "serve", "batched", "lde", "poly"])
     ap.add_argument("--serve-requests", type=int, default=20000)
     ap.add_argument("--serve-sweep", type=float, nargs="*", default=[8000.0, 32000.0])
     ap.add_argument("--serve-sweep-requests", type=int, default=6000)
@@ -621,7 +712,7 @@ def main():
         if rank == 0:
             run_serve(args)
         return
-    if args.workload in ("batched", "lde"):
+    if args.workload in ("batched", "lde", "poly"):
         if rank == 0:
             run_single_config(args)
         return

@@ -43,7 +43,9 @@ enum zntt_status {
   ZNTT_ERR_TIMEOUT = 9,            /* a bounded device wait gave up */
   ZNTT_ERR_INVALID_ARGUMENT = 10,  /* null pointer, bad handle, unknown mode */
   ZNTT_ERR_NOT_INITIALIZED = 11,   /* zntt_init() has not run */
-  ZNTT_ERR_REJECTED = 12           /* admission refused (over the memory budget / queue full) */
+  ZNTT_ERR_REJECTED = 12,          /* admission refused (over the memory budget / queue full) */
+  ZNTT_ERR_DEGREE_TOO_LARGE = 13   /* error.DegreeTooLarge: a polynomial beyond its capacity
+                                      (libs/poly/src/poly.zig:77, 200) */
 };
 
 /* ---- fields ---------------------------------------------------------------- */
@@ -142,8 +144,10 @@ int zntt_ntt_device_inplace_noalloc(const zntt_twiddles* tw, uint64_t* d_data, i
  * previous pass).  Jobs of a batch share a field and may mix sizes and kinds. */
 enum zntt_job_kind {
   ZNTT_JOB_NTT = 0,       /* nttWithTwiddles / inttWithTwiddles (libs/ntt/src/root.zig:148-212) */
-  ZNTT_JOB_COSET_LDE = 1  /* intt of 2^log_in evaluations, zero-pad, c_i *= g^i, ntt of 2^log_n:
+  ZNTT_JOB_COSET_LDE = 1, /* intt of 2^log_in evaluations, zero-pad, c_i *= g^i, ntt of 2^log_n:
                              the composition of zig-ntt with libs/poly/src/vector.zig:24-32,68-73 */
+  ZNTT_JOB_POLY_MUL = 2   /* product of two coefficient vectors (Polynomial.mul,
+                             libs/poly/src/poly.zig:197-212) through transforms of 2^log_n points */
 };
 typedef struct zntt_job {
   int kind;                   /* zntt_job_kind */
@@ -153,6 +157,11 @@ typedef struct zntt_job {
   const uint64_t* d_src;      /* 2^log_n device elements (coset extension: 2^log_in evaluations) */
   uint64_t* d_dst;            /* 2^log_n device elements; NTT jobs may transform in place */
   uint64_t shift[4];          /* coset extension: the shift g, Montgomery form */
+  const uint64_t* d_src2;     /* polynomial product: the second factor's coefficients */
+  uint64_t len, len2;         /* polynomial product: coefficient counts of d_src and d_src2, both at
+                                 least 1 with len + len2 - 1 <= 2^log_n; d_dst receives the
+                                 len + len2 - 1 product coefficients and must not overlap the
+                                 factors; tw must be the table of the primitive 2^log_n-th root */
 } zntt_job;
 typedef struct zntt_batch zntt_batch;
 
@@ -174,6 +183,32 @@ int zntt_batch_destroy(zntt_batch* b);
  * log_in / log_n are those of tw_in / tw_out. */
 int zntt_coset_lde_device(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t shift[4],
                           const uint64_t* d_evals, uint64_t* d_out, void* stream);
+
+/* ---- polynomial products -------------------------------------------------------
+ * Polynomial(F, max_degree).mul (libs/poly/src/poly.zig:197-212) computes the
+ * schoolbook product in O(deg^2).  These compute the same coefficients in
+ * O(n log n) through three transforms of n = 2^log_n >= len_a + len_b - 1 points
+ * (forward, forward with the pointwise product fused into its last pass,
+ * inverse); exact field arithmetic makes every coefficient identical. */
+
+/* d_out[0 .. len_a + len_b - 2] = the product of the coefficient vectors d_a
+ * (len_a) and d_b (len_b), with plain per-pass launches on `stream`; tw is the
+ * table of the primitive 2^log_n-th root with 2^log_n >= len_a + len_b - 1.
+ * Coefficients are not normalized (leading zeros stay).  d_out must not
+ * overlap the factors. */
+int zntt_poly_mul_device(const zntt_twiddles* tw, const uint64_t* d_a, size_t len_a, const uint64_t* d_b,
+                         size_t len_b, uint64_t* d_out, void* stream);
+
+/* Polynomial(F, max_degree).mul with host coefficient arrays: a (a_len) and b
+ * (b_len) are normalized like Polynomial.fromCoeffs (trailing zero
+ * coefficients dropped; more than max_degree + 1 coefficients is
+ * ZNTT_ERR_DEGREE_TOO_LARGE, poly.zig:76-77); a zero factor gives the zero
+ * polynomial; a product degree above max_degree is ZNTT_ERR_DEGREE_TOO_LARGE
+ * (poly.zig:198-200).  On success out[0 .. max_degree] holds the product's
+ * coefficients followed by zeros (the reference's fixed coeffs array) and
+ * *out_degree its degree, -1 for the zero polynomial.  Synchronous. */
+int zntt_poly_mul(int field, const uint64_t* a, size_t a_len, const uint64_t* b, size_t b_len, size_t max_degree,
+                  uint64_t* out, int64_t* out_degree);
 
 /* ---- serving: a continuously batching request server ---------------------------
  * Requests carry pinned host buffers.  A worker thread admits them in FIFO

@@ -32,6 +32,7 @@ INVALID_TWIDDLES = 3
 INVALID_LENGTH = 4
 OUT_OF_MEMORY = 5
 ORDER_TOO_LARGE = 6
+DEGREE_TOO_LARGE = 13
 
 MODULI = {
     BN254_FR: 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001,
@@ -83,6 +84,8 @@ def load(path: str | None = None):
     lib.zo_powers.argtypes = [i, _U64P, _U64P, sz]
     lib.zo_coset_lde.argtypes = [i, _U64P, sz, sz, _U64P, _U64P, i]
     lib.zo_dft_points.argtypes = [i, _U64P, sz, _U64P, _U64P, sz, _U64P, i]
+    lib.zo_poly_mul.argtypes = [i, _U64P, sz, _U64P, sz, sz, _U64P, ctypes.POINTER(ctypes.c_int64), i]
+    lib.zo_poly_eval.argtypes = [i, _U64P, sz, _U64P, sz, _U64P, i]
     if path.endswith("liboracle.so"):
         _lib = lib
     return lib
@@ -249,4 +252,25 @@ def dft_points(field: int, x: np.ndarray, root: np.ndarray, ks, workers: int = 1
     st = load().zo_dft_points(field, _p(np.ascontiguousarray(x)), len(x), _p(r), kk.ctypes.data_as(_U64P),
                               len(kk), _p(out), workers)
     assert st == OK
+    return out
+
+
+def poly_mul(field: int, a: np.ndarray, b: np.ndarray, max_degree: int, workers: int = 1):
+    """Polynomial(F, max_degree).fromCoeffs(a).mul(fromCoeffs(b)) by the schoolbook loops of
+    libs/poly/src/poly.zig:197-212: (status, coefficients[max_degree + 1], degree)."""
+    out = elems(max_degree + 1)
+    deg = ctypes.c_int64(0)
+    na, nb = len(a), len(b)
+    a = np.ascontiguousarray(a.reshape(-1, 4)) if na else elems(1)
+    b = np.ascontiguousarray(b.reshape(-1, 4)) if nb else elems(1)
+    st = load().zo_poly_mul(field, _p(a), na, _p(b), nb, max_degree, _p(out), ctypes.byref(deg), workers)
+    return st, out, deg.value
+
+
+def poly_eval(field: int, c: np.ndarray, xs: np.ndarray, workers: int = 1) -> np.ndarray:
+    """Horner evaluation of the coefficients c at each point of xs (poly.zig:214-224)."""
+    out = elems(len(xs))
+    st = load().zo_poly_eval(field, _p(np.ascontiguousarray(c)), len(c), _p(np.ascontiguousarray(xs)), len(xs),
+                             _p(out), workers)
+    assert st == OK, st
     return out

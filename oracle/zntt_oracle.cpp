@@ -21,6 +21,7 @@
 //   libs/rng/src/chacha20.zig:36-160       ChaCha20 block function and keystream
 //   libs/rng/src/rng.zig:32-65             randomFieldElement (big-endian rejection draw)
 //   libs/poly/src/vector.zig:24-32,68-73   powers / hadamard (coset LDE composition)
+//   libs/poly/src/poly.zig:76-107,197-224  fromCoeffs / normalize / mul (schoolbook) / eval
 //   libs/parallel/src/root.zig:45-79       parallelFor fork-join semantics (harness only)
 //
 // The reference is Zig 0.16 and cannot be compiled in this environment; the
@@ -52,6 +53,7 @@ enum {
   ZO_UNSUPPORTED_FIELD = 7,
   ZO_REJECTION_FAILED = 8,
   ZO_INVERSE_OF_ZERO = 9,
+  ZO_DEGREE_TOO_LARGE = 13,  // libs/poly/src/poly.zig:77, 200 (same number as the product's code)
 };
 
 enum {
@@ -1046,6 +1048,79 @@ int zo_dft_points(int field, const uint64_t* x, size_t n, const uint64_t* root, 
           F.mul(acc, z, t);
           load<N>(x + 4 * j, xi);
           F.add(t, xi, acc);
+        }
+        store<N>(out + 4 * q, acc);
+      }
+    });
+    return ZO_OK;
+  });
+}
+
+// Polynomial(F, max_degree) over coefficient arrays: fromCoeffs
+// (libs/poly/src/poly.zig:76-84: more than max_degree + 1 coefficients is
+// DegreeTooLarge, then normalize), normalize (:100-104: degree = index of the
+// last non-zero coefficient, -1 for zero) and mul (:197-212: a zero factor
+// gives zero; a product degree above max_degree is DegreeTooLarge; else
+// r[i + j] += a_i * b_j for every pair, in the reference's order: i outer, j
+// inner, then normalize).  out receives max_degree + 1 coefficients.  The
+// harness splits the output coefficients over `workers` threads; each
+// coefficient still accumulates its products in increasing i, as the
+// reference's loops do for it.
+int zo_poly_mul(int field, const uint64_t* a, size_t a_len, const uint64_t* b, size_t b_len, size_t max_degree,
+                uint64_t* out, int64_t* out_degree, int workers) {
+  return dispatch(field, [&](const auto& F) -> int {
+    constexpr int N = sizeof(F.P) / sizeof(uint64_t);
+    if (a_len > max_degree + 1 || b_len > max_degree + 1) return ZO_DEGREE_TOO_LARGE;
+    auto degree = [&](const uint64_t* c, size_t len) -> int64_t {
+      int64_t d = (int64_t)len - 1;
+      while (d >= 0) {
+        uint64_t x[N];
+        load<N>(c + 4 * d, x);
+        bool zero = true;
+        for (int q = 0; q < N; q++) zero = zero && x[q] == 0;
+        if (!zero) break;
+        d--;
+      }
+      return d;
+    };
+    const int64_t da = degree(a, a_len), db = degree(b, b_len);
+    std::memset(out, 0, (max_degree + 1) * 32);
+    if (da < 0 || db < 0) {
+      *out_degree = -1;
+      return ZO_OK;
+    }
+    const int64_t d = da + db;
+    if ((uint64_t)d > max_degree) return ZO_DEGREE_TOO_LARGE;
+    Vec<N> va = unpack<N>(a, (size_t)da + 1), vb = unpack<N>(b, (size_t)db + 1);
+    parallel_for((size_t)d + 1, workers, [&](size_t lo, size_t hi) {
+      for (size_t k = lo; k < hi; k++) {
+        uint64_t acc[N] = {0}, t[N];
+        const size_t i0 = k > (size_t)db ? k - (size_t)db : 0, i1 = std::min(k, (size_t)da);
+        for (size_t i = i0; i <= i1; i++) {
+          F.mul(va[i].l, vb[k - i].l, t);
+          F.add(acc, t, acc);
+        }
+        store<N>(out + 4 * k, acc);
+      }
+    });
+    *out_degree = degree(out, (size_t)d + 1);
+    return ZO_OK;
+  });
+}
+
+// Horner evaluation of c (len coefficients) at each of m points
+// (Polynomial.eval, libs/poly/src/poly.zig:214-224).
+int zo_poly_eval(int field, const uint64_t* c, size_t len, const uint64_t* xs, size_t m, uint64_t* out, int workers) {
+  return dispatch(field, [&](const auto& F) -> int {
+    constexpr int N = sizeof(F.P) / sizeof(uint64_t);
+    parallel_for(m, workers, [&](size_t lo, size_t hi) {
+      for (size_t q = lo; q < hi; q++) {
+        uint64_t z[N], acc[N] = {0}, t[N], ci[N];
+        load<N>(xs + 4 * q, z);
+        for (size_t j = len; j-- > 0;) {
+          F.mul(acc, z, t);
+          load<N>(c + 4 * j, ci);
+          F.add(t, ci, acc);
         }
         store<N>(out + 4 * q, acc);
       }

@@ -17,6 +17,10 @@ Two kinds of fixture:
      checked against the definition (n = 2^12, the plain 2^12 BN254-Fr case).
    * coset_lde.json -- a small blowup-4 coset extension over BLS12-381-Fr with
      shift 5, the reference's quadratic non-residue.
+   * poly_mul.json -- polynomial products by the schoolbook sum over both
+     fields: seeded factors of several lengths, trailing zero coefficients
+     (normalized away), a zero factor, constants, and max_degree cases that
+     fit exactly or raise DegreeTooLarge.
 
 Values are canonical (not Montgomery) hex strings.  Large vectors are stored as
 a SHA-256 of their little-endian 32-byte encoding plus a few leading values.
@@ -128,6 +132,38 @@ def lde_case() -> dict:
             "shift": shift, "evals": [hex(v) for v in evals], "output": [hex(v) for v in out]}
 
 
+def poly_cases() -> list[dict]:
+    out = []
+    plan = [("bn254_fr", pyref.BN254_FR_P, 404), ("bls12_381_fr", pyref.BLS12_381_FR_P, 505)]
+    shapes = [(1, 1), (1, 7), (5, 3), (16, 16), (33, 17), (64, 1), (100, 57)]
+    for name, p, seed0 in plan:
+        for q, (la, lb) in enumerate(shapes):
+            a = pyref.random_field_values(p, seed0 + 2 * q, la)
+            b = pyref.random_field_values(p, seed0 + 2 * q + 1, lb)
+            c = pyref.poly_mul(a, b, p)
+            d = len(c) - 1
+            out.append({"field": name, "a": [hex(v) for v in a], "b": [hex(v) for v in b],
+                        "max_degree": d + 3, "degree": d, "product": [hex(v) for v in c]})
+        # Trailing zeros in the inputs are dropped; the product has exactly max_degree.
+        a = pyref.random_field_values(p, seed0 + 50, 6) + [0, 0]
+        b = pyref.random_field_values(p, seed0 + 51, 4) + [0]
+        c = pyref.poly_mul(a, b, p)
+        out.append({"field": name, "a": [hex(v) for v in a], "b": [hex(v) for v in b],
+                    "max_degree": len(c) - 1, "degree": len(c) - 1, "product": [hex(v) for v in c]})
+        # One degree short of fitting: DegreeTooLarge.
+        out.append({"field": name, "a": [hex(v) for v in a], "b": [hex(v) for v in b],
+                    "max_degree": len(c) - 2, "error": "DegreeTooLarge"})
+        # A factor with more coefficients than the capacity: DegreeTooLarge (fromCoeffs).
+        out.append({"field": name, "a": [hex(v) for v in a], "b": ["0x1"], "max_degree": len(a) - 2,
+                    "error": "DegreeTooLarge"})
+        # A zero factor (all coefficients zero, or none): the zero polynomial.
+        out.append({"field": name, "a": ["0x0", "0x0"], "b": [hex(v) for v in b], "max_degree": 10,
+                    "degree": -1, "product": []})
+        out.append({"field": name, "a": [], "b": [hex(v) for v in b], "max_degree": 10, "degree": -1,
+                    "product": []})
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -136,6 +172,7 @@ def main() -> None:
     json.dump(parse_rfc(args.reference), open(os.path.join(HERE, "chacha20_rfc8439.json"), "w"), indent=1)
     json.dump(fr_cases(), open(os.path.join(HERE, "fr_transforms.json"), "w"), indent=1)
     json.dump(lde_case(), open(os.path.join(HERE, "coset_lde.json"), "w"), indent=1)
+    json.dump(poly_cases(), open(os.path.join(HERE, "poly_mul.json"), "w"), indent=1)
     print("fixtures written to", HERE)
 
 

@@ -10,6 +10,9 @@ the three is evidence rather than self-consistency:
   reference's known-answer test pins, libs/ntt/src/root.zig:399-453), plus a
   recursive radix-2 FFT over Python integers for sizes where the O(n^2) sum is
   too slow; the FFT is checked against the definition at small sizes.
+* Polynomial products by the schoolbook sum c_k = sum_{i+j=k} a_i b_j over
+  Python integers (what Polynomial.mul of libs/poly/src/poly.zig:197-212
+  computes), with the reference's degree convention (-1 for zero).
 * Roots of unity as the reference derives them (libs/field/src/roots.zig:149-158):
   z = the first quadratic non-residue counting up from 2, raised to
   odd_part << (two_adicity - log_n).
@@ -141,3 +144,22 @@ def coset_lde(evals: list[int], log_blowup: int, shift: int, p: int) -> list[int
         padded[i] = padded[i] * g % p
         g = g * shift % p
     return fft(padded, primitive_root(p, log_in + log_blowup), p)
+
+
+def degree(c: list[int]) -> int:
+    d = len(c) - 1
+    while d >= 0 and c[d] == 0:
+        d -= 1
+    return d
+
+
+def poly_mul(a: list[int], b: list[int], p: int) -> list[int]:
+    """The product's coefficients (degree deg a + deg b), [] when a factor is zero."""
+    da, db = degree(a), degree(b)
+    if da < 0 or db < 0:
+        return []
+    c = [0] * (da + db + 1)
+    for i in range(da + 1):
+        for j in range(db + 1):
+            c[i + j] = (c[i + j] + a[i] * b[j]) % p
+    return c

@@ -90,3 +90,28 @@ def test_unsupported_field_rejected(zntt):
     bogus = zntt.Field(9, "bogus", 7, 1)
     with pytest.raises(zntt.UnsupportedField):
         zntt.ntt(bogus, np.zeros((2, 4), dtype=np.uint64), 1, np.zeros(4, dtype=np.uint64))
+
+
+def test_poly_mul_contract_before_any_device_work(zntt, oracle):
+    """Polynomial.mul's results that need no transform (libs/poly/src/poly.zig:76-77, 198-200):
+    a zero factor is the zero polynomial, and both DegreeTooLarge cases are raised before the
+    library looks for a device."""
+    for F, fid in ((zntt.BN254_FR, O.BN254_FR), (zntt.BLS12_381_FR, O.BLS12_381_FR)):
+        b = O.random_elements(fid, 9, 4)
+        for a in (np.zeros((3, 4), dtype=np.uint64), np.zeros((0, 4), dtype=np.uint64)):
+            out, deg = zntt.poly_mul(F, a, b, 10)
+            assert deg == -1 and not out.any() and out.shape == (11, 4)
+        a = O.random_elements(fid, 10, 6)
+        with pytest.raises(zntt.DegreeTooLarge):
+            zntt.poly_mul(F, a, b, 7)  # product degree 8 > 7
+        with pytest.raises(zntt.DegreeTooLarge):
+            zntt.poly_mul(F, a, b[:1], 4)  # six coefficients do not fit max_degree 4
+        # fromCoeffs checks the length before it normalizes: seven coefficients do not fit
+        # max_degree 4 even when six of them are zero and the product (degree 2) would.
+        padded = np.concatenate([b[:1], np.zeros((6, 4), dtype=np.uint64)])
+        with pytest.raises(zntt.DegreeTooLarge):
+            zntt.poly_mul(F, a[:3], padded, 4)
+    with pytest.raises(zntt.UnsupportedField):
+        zntt._check(zntt.lib().zntt_poly_mul(5, None, 0, None, 0, 0, None, None))
+    with pytest.raises(zntt.InvalidArgument):
+        zntt._check(zntt.lib().zntt_poly_mul(0, None, 2, None, 0, 4, None, None))

@@ -267,3 +267,42 @@ def test_parallel_harness_matches_single_thread():
     np.testing.assert_array_equal(a, b)
     O.ntt_with_twiddles(f, b, log_n, tw, inverse=True, workers=3, inplace4=True)
     np.testing.assert_array_equal(b, x)
+
+
+def _poly_fixture_inputs(c):
+    f = FIELD_IDS[c["field"]]
+    a = _mont_of(f, [int(v, 16) for v in c["a"]]) if c["a"] else O.elems(0)
+    b = _mont_of(f, [int(v, 16) for v in c["b"]]) if c["b"] else O.elems(0)
+    return f, a, b
+
+
+def test_poly_mul_fixture():
+    """The schoolbook product (libs/poly/src/poly.zig:197-212) against the independent
+    pure-Python sum, with the reference's normalisation, zero and DegreeTooLarge cases."""
+    for c in json.load(open(os.path.join(GOLDEN, "poly_mul.json"))):
+        f, a, b = _poly_fixture_inputs(c)
+        st, out, deg = O.poly_mul(f, a, b, c["max_degree"], workers=4)
+        if "error" in c:
+            assert st == O.DEGREE_TOO_LARGE, c
+            continue
+        assert st == O.OK and deg == c["degree"], (st, deg, c["degree"])
+        got = _canon_ints(f, out)
+        want = [int(v, 16) for v in c["product"]]
+        assert got[:len(want)] == want
+        assert all(v == 0 for v in got[len(want):])
+
+
+def test_poly_mul_evaluates_to_the_product_of_evaluations():
+    """c(x) = a(x) b(x) at random points (Polynomial.eval, poly.zig:214-224), for sizes the
+    fixture does not reach, and one thread vs several give the same coefficients."""
+    for f in (O.BN254_FR, O.BLS12_381_FR):
+        a = O.random_elements(f, 71, 700)
+        b = O.random_elements(f, 72, 333)
+        st, c1, d = O.poly_mul(f, a, b, 1100, workers=1)
+        st4, c4, d4 = O.poly_mul(f, a, b, 1100, workers=8)
+        assert st == st4 == O.OK and d == d4 == 1031
+        np.testing.assert_array_equal(c1, c4)
+        x = O.random_elements(f, 73, 8)
+        lhs = O.poly_eval(f, c1[:d + 1], x)
+        rhs = O.elementwise(f, "mul", O.poly_eval(f, a, x), O.poly_eval(f, b, x))
+        np.testing.assert_array_equal(lhs, rhs)

@@ -86,9 +86,14 @@ class Rejected(ZnttError):
     code = 12
 
 
+class DegreeTooLarge(ZnttError):
+    """error.DegreeTooLarge of libs/poly/src/poly.zig:77, 200."""
+    code = 13
+
+
 _ERRORS = {c.code: c for c in (LogTooLarge, LengthMismatch, InvalidTwiddles, InvalidLength, OutOfMemory,
                                OrderTooLarge, UnsupportedField, DeviceError, Timeout, InvalidArgument,
-                               NotInitialized, Rejected)}
+                               NotInitialized, Rejected, DegreeTooLarge)}
 
 
 # --- fields ----------------------------------------------------------------------
@@ -122,6 +127,7 @@ _lib = None
 
 JOB_NTT = 0
 JOB_COSET_LDE = 1
+JOB_POLY_MUL = 2
 
 
 class ServerConfig(ctypes.Structure):
@@ -155,7 +161,8 @@ class Job(ctypes.Structure):
     """zntt_job (include/zntt.h)."""
     _fields_ = [("kind", ctypes.c_int), ("mode", ctypes.c_int), ("tw", ctypes.c_void_p),
                 ("tw_in", ctypes.c_void_p), ("d_src", ctypes.c_void_p), ("d_dst", ctypes.c_void_p),
-                ("shift", ctypes.c_uint64 * 4)]
+                ("shift", ctypes.c_uint64 * 4), ("d_src2", ctypes.c_void_p), ("len", ctypes.c_uint64),
+                ("len2", ctypes.c_uint64)]
 _device = None
 
 
@@ -196,6 +203,8 @@ def lib():
                                       ctypes.POINTER(i), ctypes.POINTER(i)]
         L.zntt_batch_destroy.argtypes = [vp]
         L.zntt_coset_lde_device.argtypes = [vp, vp, _U64P, vp, vp, vp]
+        L.zntt_poly_mul_device.argtypes = [vp, vp, sz, vp, sz, vp, vp]
+        L.zntt_poly_mul.argtypes = [i, _U64P, sz, _U64P, sz, sz, _U64P, ctypes.POINTER(ctypes.c_int64)]
         L.zntt_autotune.argtypes = [i, ctypes.c_uint32, ctypes.c_uint32]
         L.zntt_tune_save.argtypes = [ctypes.c_char_p]
         L.zntt_tune_load.argtypes = [ctypes.c_char_p]
@@ -452,8 +461,9 @@ class Batch:
 
     `jobs` is a list of dicts: {"kind": JOB_NTT, "tw": DeviceTwiddles, "mode": FORWARD,
     "src": ptr, "dst": ptr} or {"kind": JOB_COSET_LDE, "tw": out table, "tw_in": in table,
-    "shift": 4 Montgomery limbs, "src": ptr, "dst": ptr}.  Device buffers stay owned by the
-    caller and must outlive the batch."""
+    "shift": 4 Montgomery limbs, "src": ptr, "dst": ptr} or {"kind": JOB_POLY_MUL, "tw": table of
+    2^log_n >= len + len2 - 1 points, "src": ptr, "len": n, "src2": ptr, "len2": m, "dst": ptr to
+    len + len2 - 1 elements}.  Device buffers stay owned by the caller and must outlive the batch."""
 
     def __init__(self, F: Field, jobs, shape: int = -1):
         _ensure_init()
@@ -468,6 +478,9 @@ class Batch:
             if "shift" in j:
                 for k, v in enumerate(np.asarray(j["shift"], dtype=np.uint64).reshape(4)):
                     arr[i].shift[k] = int(v)
+            arr[i].d_src2 = j.get("src2")
+            arr[i].len = j.get("len", 0)
+            arr[i].len2 = j.get("len2", 0)
         h = ctypes.c_void_p()
         _check(lib().zntt_batch_create(F.id, arr, len(jobs), shape, ctypes.byref(h)))
         self.handle = h
@@ -502,6 +515,31 @@ def coset_lde_device(tw_in: DeviceTwiddles, tw_out: DeviceTwiddles, shift, d_eva
                      stream: int = 0) -> None:
     """One coset low-degree extension with plain per-pass launches."""
     _check(lib().zntt_coset_lde_device(tw_in.handle, tw_out.handle, _root(shift), d_evals, d_out, stream or None))
+
+
+def poly_mul_device(tw: DeviceTwiddles, d_a: int, len_a: int, d_b: int, len_b: int, d_out: int,
+                    stream: int = 0) -> None:
+    """d_out[0 .. len_a + len_b - 2] = the product of two device coefficient vectors
+    (zntt_poly_mul_device); tw is the table of a primitive 2^log_n-th root with
+    2^log_n >= len_a + len_b - 1."""
+    _check(lib().zntt_poly_mul_device(tw.handle, d_a, len_a, d_b, len_b, d_out, stream or None))
+
+
+def poly_mul(F: Field, a: np.ndarray, b: np.ndarray, max_degree: int):
+    """Polynomial(F, max_degree).fromCoeffs(a).mul(fromCoeffs(b)) (libs/poly/src/poly.zig:76-84,
+    197-212) on the device: returns (coefficients, an (max_degree + 1, 4) uint64 array of
+    Montgomery limbs, zero beyond the degree; degree, -1 for the zero polynomial).  Raises
+    DegreeTooLarge as the reference does."""
+    _ensure_init()
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.uint64).reshape(-1, 4))
+    b = np.ascontiguousarray(np.asarray(b, dtype=np.uint64).reshape(-1, 4))
+    out = np.zeros((max_degree + 1, 4), dtype=np.uint64)
+    deg = ctypes.c_int64(0)
+    pa = a.ctypes.data_as(_U64P) if len(a) else None
+    pb = b.ctypes.data_as(_U64P) if len(b) else None
+    _check(lib().zntt_poly_mul(F.id, pa, len(a), pb, len(b), max_degree, out.ctypes.data_as(_U64P),
+                               ctypes.byref(deg)))
+    return out, deg.value
 
 
 def autotune(F: Field, log_n_min: int, log_n_max: int) -> None:

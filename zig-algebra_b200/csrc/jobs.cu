@@ -100,7 +100,8 @@ static PassParams pass_params(const TwEntry* tw, uint32_t log_n, const PassDesc&
   pp.first = first;
   pp.inverse = inverse;
   pp.tw0_one = tw->tw0_one;
-  pp.src_log = log_n;
+  pp.src_len = 1ull << log_n;
+  pp.dst_len = 1ull << log_n;
   return pp;
 }
 
@@ -119,11 +120,12 @@ Plan batch_plan(int field, uint32_t log_n, int shape) {
 // first run in place).
 void plan_transform(JobPlan& jp, const TwEntry* tw, const Plan& plan, uint32_t log_n, const uint4* src,
                            uint4* mid, uint4* dst, bool inverse, const uint64_t* scale_val, const uint4* scale_tab,
-                           uint32_t src_log) {
+                           uint64_t src_len, uint64_t dst_len) {
   for (uint32_t p = 0; p < plan.np; p++) {
     const bool first = p == 0, last = p + 1 == plan.np;
     PassParams pp = pass_params(tw, log_n, plan.p[p], first, inverse, first ? src : mid, last ? dst : mid);
-    if (first) pp.src_log = src_log;
+    if (first) pp.src_len = src_len;
+    if (last) pp.dst_len = dst_len;
     if (last && (scale_val || scale_tab)) {
       pp.scale = 1;
       if (scale_val) std::memcpy(pp.scale_val, scale_val, 32);
@@ -133,6 +135,23 @@ void plan_transform(JobPlan& jp, const TwEntry* tw, const Plan& plan, uint32_t l
     jp.tiles.push_back((1ull << log_n) >> (plan.p[p].k + plan.p[p].c));
     jp.work += ((size_t)1 << log_n) * plan.p[p].k;
   }
+}
+
+// Polynomial.mul (libs/poly/src/poly.zig:197-212) computes the product
+// coefficients c_k = sum_{i+j=k} a_i b_j directly.  With 2^log_n >= len_a +
+// len_b - 1 points the cyclic convolution of the zero-padded inputs is that
+// linear product, and by the convolution theorem it is
+// intt(ntt(a) . ntt(b)).  Field arithmetic is exact, so every coefficient is
+// the schoolbook sum's canonical value.
+void plan_poly_mul(JobPlan& jp, const TwEntry* tw, const Plan& plan, const uint4* a, uint64_t len_a, const uint4* b,
+                   uint64_t len_b, uint4* s1, uint4* s2, uint4* dst) {
+  const uint32_t L = tw->log_n;
+  const uint64_t n = 1ull << L;
+  uint64_t ninv[4];
+  n_inverse(tw->field, L, ninv);
+  plan_transform(jp, tw, plan, L, a, s1, s1, false, nullptr, nullptr, len_a, n);
+  plan_transform(jp, tw, plan, L, b, s2, s2, false, nullptr, s1, len_b, n);
+  plan_transform(jp, tw, plan, L, s2, s1, dst, true, ninv, nullptr, n, len_a + len_b - 1);
 }
 
 }  // namespace zntt
@@ -195,6 +214,13 @@ int zntt_batch_create(int field, const zntt_job* jobs, size_t n_jobs, int shape,
       if (tw_of(job.tw_in)->log_n > tw_of(job.tw)->log_n)
         return set_error(ZNTT_ERR_INVALID_ARGUMENT, "coset extension shrinks the vector");
       if (job.d_src == job.d_dst) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "coset extension in place");
+    } else if (job.kind == ZNTT_JOB_POLY_MUL) {
+      const uint64_t n = 1ull << tw_of(job.tw)->log_n;
+      if (!job.d_src2) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "polynomial product without a second factor");
+      if (job.len < 1 || job.len2 < 1 || job.len > n || job.len2 > n || job.len + job.len2 - 1 > n)
+        return set_error(ZNTT_ERR_INVALID_ARGUMENT, "polynomial product does not fit the transform size");
+      if (job.d_dst == job.d_src || job.d_dst == job.d_src2)
+        return set_error(ZNTT_ERR_INVALID_ARGUMENT, "polynomial product into a factor");
     } else {
       return set_error(ZNTT_ERR_INVALID_ARGUMENT, "unknown job kind");
     }
@@ -228,7 +254,22 @@ int zntt_batch_create(int field, const zntt_job* jobs, size_t n_jobs, int shape,
       uint64_t ninv[4];
       const bool inv = job.mode == ZNTT_INVERSE;
       if (inv) n_inverse(field, L, ninv);
-      plan_transform(plans[j], tw, plan, L, src, mid, dst, inv, inv ? ninv : nullptr, nullptr, L);
+      plan_transform(plans[j], tw, plan, L, src, mid, dst, inv, inv ? ninv : nullptr, nullptr, 1ull << L, 1ull << L);
+    } else if (job.kind == ZNTT_JOB_POLY_MUL) {
+      void* s1 = nullptr;
+      void* s2 = nullptr;
+      int rc = pool_get((size_t)32 << L, &s1);
+      if (!rc) {
+        b->scratch.push_back({s1, (size_t)32 << L});
+        rc = pool_get((size_t)32 << L, &s2);
+      }
+      if (rc) {
+        free_batch(b);
+        return rc;
+      }
+      b->scratch.push_back({s2, (size_t)32 << L});
+      plan_poly_mul(plans[j], tw, batch_plan(field, L, b->shape), src, job.len,
+                    reinterpret_cast<const uint4*>(job.d_src2), job.len2, (uint4*)s1, (uint4*)s2, dst);
     } else {
       const TwEntry* twi = tw_of(job.tw_in);
       const uint32_t Li = twi->log_n;
@@ -248,8 +289,10 @@ int zntt_batch_create(int field, const zntt_job* jobs, size_t n_jobs, int shape,
       b->scratch.push_back({coef, (size_t)32 << Li});
       const Plan pin = batch_plan(field, Li, b->shape);
       const Plan pout = batch_plan(field, L, b->shape);
-      plan_transform(plans[j], twi, pin, Li, src, (uint4*)coef, (uint4*)coef, true, nullptr, ct->d, Li);
-      plan_transform(plans[j], tw, pout, L, (const uint4*)coef, dst, dst, false, nullptr, nullptr, Li);
+      plan_transform(plans[j], twi, pin, Li, src, (uint4*)coef, (uint4*)coef, true, nullptr, ct->d, 1ull << Li,
+                     1ull << Li);
+      plan_transform(plans[j], tw, pout, L, (const uint4*)coef, dst, dst, false, nullptr, nullptr, 1ull << Li,
+                     1ull << L);
     }
   }
 
@@ -394,9 +437,9 @@ int zntt_coset_lde_device(const zntt_twiddles* tw_in, const zntt_twiddles* tw_ou
   const Plan pin = tuned_plan(ti->field, ti->log_n);
   const Plan pout = tuned_plan(to->field, to->log_n);
   plan_transform(jp, ti, pin, ti->log_n, (const uint4*)d_evals, (uint4*)coef, (uint4*)coef, true, nullptr, ct->d,
-                 ti->log_n);
+                 1ull << ti->log_n, 1ull << ti->log_n);
   plan_transform(jp, to, pout, to->log_n, (const uint4*)coef, (uint4*)d_out, (uint4*)d_out, false, nullptr, nullptr,
-                 ti->log_n);
+                 1ull << ti->log_n, 1ull << to->log_n);
   cudaError_t ce = cudaSuccess;
   for (size_t p = 0; p < jp.passes.size() && ce == cudaSuccess; p++) {
     const int shape = p < pin.np ? pin.shape : pout.shape;

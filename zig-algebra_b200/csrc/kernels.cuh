@@ -33,8 +33,9 @@ struct PassParams {
   uint32_t tw0_one;   // every stage's entry 0 is one (j = 0 needs no multiply)
   uint32_t scale;     // multiply each output by scale_val (or scale_tab[q]) after the last stage
   uint32_t scale_val[8];
-  uint32_t src_log;   // first pass: natural input index >= 2^src_log reads as zero (zero padding)
   const uint4* scale_tab;  // when non-null, output position q is scaled by scale_tab[q]
+  uint64_t src_len;   // first pass: natural input index >= src_len reads as zero (zero padding)
+  uint64_t dst_len;   // output positions >= dst_len are not stored
 };
 
 // Pass kernel shapes.  Each shape is a compiled kernel: a tile of 2^log_tile
@@ -51,10 +52,11 @@ constexpr int kDefaultShape = 0;
 
 inline int shape_smem_bytes(int shape) { return (1 << kShapes[shape].log_tile) * 32; }
 
-// A pass that pads its input with zeros or scales by a table runs the
-// extension variant of the kernels.
+// A pass that pads its input with zeros, scales by a table or stores a prefix
+// of its output runs the extension variant of the kernels.
 inline bool pass_needs_ext(const PassParams& pp) {
-  return (pp.first && pp.src_log < pp.log_n) || (pp.scale && pp.scale_tab != nullptr);
+  const uint64_t n = 1ull << pp.log_n;
+  return (pp.first && pp.src_len < n) || (pp.scale && pp.scale_tab != nullptr) || pp.dst_len < n;
 }
 
 cudaError_t launch_ntt_pass(int field, int shape, const PassParams& pp, uint64_t num_tiles, cudaStream_t st);

@@ -123,7 +123,8 @@ extern "C" int zntt_ntt_device_inplace_noalloc(const zntt_twiddles* tw, uint64_t
     pp.tw0_one = e->tw0_one;
     pp.scale = last && inverse;
     if (pp.scale) std::memcpy(pp.scale_val, ninv, 32);
-    pp.src_log = log_n;
+    pp.src_len = 1ull << log_n;
+    pp.dst_len = 1ull << log_n;
     const uint64_t tiles = (1ull << log_n) >> (pp.k + pp.c);
     ce = launch_ntt_pass(e->field, kDefaultShape, pp, tiles, st);
     if (ce != cudaSuccess) return cuda_fail(ce, "ntt pass launch");

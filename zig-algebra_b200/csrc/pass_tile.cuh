@@ -80,9 +80,10 @@ __device__ __forceinline__ uint4 load_data(const uint4* p) {
   else return *p;
 }
 
-// EXT enables the coset-extension features: zero padding of the first pass's
-// input beyond 2^src_log and a per-position scale table.  Plain transforms
-// compile without them (fewer live registers in the hot loop).
+// EXT enables the extension features: zero padding of the first pass's input
+// from index src_len, a per-position scale table, and storing only the output
+// positions below dst_len.  Plain transforms compile without them (fewer live
+// registers in the hot loop).
 template <class F, int LOG_TILE, int THREADS, bool COHERENT, bool EXT>
 __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uint4* sm) {
   constexpr uint32_t TILE_MAX = 1u << LOG_TILE;
@@ -99,7 +100,7 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
     m0 = (blk & ((1ull << mlog) - 1)) << c;
   }
   const uint32_t xcols_log = pp.log_n - k;
-  const uint64_t src_len = 1ull << pp.src_log;
+  const uint64_t src_len = pp.src_len;
 
   // ---- load: column-fastest, 16-byte halves ----
 #pragma unroll
@@ -229,7 +230,7 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
       } else {
         g = hi_base + ((uint64_t)row << pp.S) + m0 + col;
       }
-      pp.dst[(g << 1) | h] = sm[h * TILE_MAX + ((row << c) | col)];
+      if (!EXT || g < pp.dst_len) pp.dst[(g << 1) | h] = sm[h * TILE_MAX + ((row << c) | col)];
     }
   }
 }

@@ -172,7 +172,8 @@ int run_plan(int field, const TwEntry* tw, const Plan& plan, uint32_t log_n, con
     pp.tw0_one = tw->tw0_one;
     pp.scale = last && scale;
     if (pp.scale) std::memcpy(pp.scale_val, scale_val, 32);
-    pp.src_log = log_n;
+    pp.src_len = 1ull << log_n;
+    pp.dst_len = 1ull << log_n;
     const uint64_t tiles = (1ull << log_n) >> (d.k + d.c);
     ZCHECK(launch_ntt_pass(field, plan.shape, pp, tiles, st), "ntt pass launch");
     cur_src = pp.dst;

@@ -261,7 +261,7 @@ static bool launch_into(zntt_server* s, Slot& sl) {
       if (inv) n_inverse(field, r.log_n, ninv);
       const Plan plan = s->cfg.serial ? tuned_plan(field, r.log_n) : batch_plan(field, r.log_n, shape);
       plan_transform(plans[j], tw, plan, r.log_n, (const uint4*)q.d_in, (uint4*)q.d_out, (uint4*)q.d_out, inv,
-                     inv ? ninv : nullptr, nullptr, r.log_n);
+                     inv ? ninv : nullptr, nullptr, 1ull << r.log_n, 1ull << r.log_n);
     } else {
       TwEntry* twi = nullptr;
       rc = table_for(s, r.log_in, &twi);
@@ -273,9 +273,9 @@ static bool launch_into(zntt_server* s, Slot& sl) {
       const Plan pi = s->cfg.serial ? tuned_plan(field, r.log_in) : batch_plan(field, r.log_in, shape);
       const Plan po = s->cfg.serial ? tuned_plan(field, r.log_n) : batch_plan(field, r.log_n, shape);
       plan_transform(plans[j], twi, pi, r.log_in, (const uint4*)q.d_in, (uint4*)q.d_coef, (uint4*)q.d_coef, true,
-                     nullptr, q.ct->d, r.log_in);
+                     nullptr, q.ct->d, 1ull << r.log_in, 1ull << r.log_in);
       plan_transform(plans[j], tw, po, r.log_n, (const uint4*)q.d_coef, (uint4*)q.d_out, (uint4*)q.d_out, false,
-                     nullptr, nullptr, r.log_in);
+                     nullptr, nullptr, 1ull << r.log_in, 1ull << r.log_n);
     }
   }
 
