@@ -25,6 +25,7 @@ extern fn zntt_precompute_twiddles(field: c_int, log_n: usize, root: *const [4]u
 extern fn zntt_free_twiddles(field: c_int, stages: [*]const ZStage, num_stages: usize) void;
 extern fn zntt_ntt_with_twiddles(field: c_int, data: [*]u64, len: usize, log_n: usize, stages: [*]const ZStage, num_stages: usize) c_int;
 extern fn zntt_intt_with_twiddles(field: c_int, data: [*]u64, len: usize, log_n: usize, stages: [*]const ZStage, num_stages: usize) c_int;
+extern fn zntt_poly_mul(field: c_int, a: [*]const u64, a_len: usize, b: [*]const u64, b_len: usize, max_degree: usize, out: [*]u64, out_degree: *i64) c_int;
 
 const BN254_FR: u512 = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001;
 const BLS12_381_FR: u512 = 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001;
@@ -158,4 +159,24 @@ pub fn nttWithTwiddles(comptime F: type, data: []F, log_n: usize, twiddles: []co
 
 pub fn inttWithTwiddles(comptime F: type, data: []F, log_n: usize, twiddles: []const []const F) error{ LogTooLarge, LengthMismatch, InvalidTwiddles, InvalidLength, DeviceError, OutOfMemory }!void {
     return withTwiddles(F, data, log_n, twiddles, true);
+}
+
+/// `Polynomial(F, max_degree).mul` (libs/poly/src/poly.zig:197-212) on the GPU, for zig-poly
+/// to call in place of its schoolbook loop when the degrees are large.  `P` is the
+/// `Polynomial(F, max_degree)` type (fields `coeffs: [MAX_DEGREE + 1]F` and `degree: i32`);
+/// the result is the same value, normalized, with the same `DegreeTooLarge` rule.
+pub fn polyMul(comptime P: type, a: P, b: P) error{ DegreeTooLarge, DeviceError, OutOfMemory }!P {
+    const F = @TypeOf(a.coeffs[0]);
+    const id = fieldId(F);
+    if (a.degree < 0 or b.degree < 0) return P.zero();
+    if (a.degree + b.degree > P.MAX_DEGREE) return error.DegreeTooLarge;
+    try ensureInit();
+    var r = P.zero();
+    var deg: i64 = -1;
+    const status = zntt_poly_mul(id, @ptrCast(&a.coeffs), @intCast(a.degree + 1), @ptrCast(&b.coeffs),
+        @intCast(b.degree + 1), P.MAX_DEGREE, @ptrCast(&r.coeffs), &deg);
+    if (status == 13) return error.DegreeTooLarge;
+    try @as(DeviceFailure!void, @errorCast(mapStatus(status)));
+    r.degree = @intCast(deg);
+    return r;
 }
