@@ -51,7 +51,18 @@ enum zntt_status {
 /* ---- fields ---------------------------------------------------------------- */
 enum zntt_field {
   ZNTT_FIELD_BN254_FR = 0,      /* r = 0x30644e72...43e1f593f0000001, two-adicity 28 */
-  ZNTT_FIELD_BLS12_381_FR = 1   /* r = 0x73eda753...ffffffff00000001, two-adicity 32 */
+  ZNTT_FIELD_BLS12_381_FR = 1,  /* r = 0x73eda753...ffffffff00000001, two-adicity 32 */
+  /* zig-field's SmallField backend (libs/field/src/field.zig:89-849), the fields of the
+   * reference's own transform known-answer tests (libs/ntt/src/root.zig:437-447).  An element
+   * is SmallField's canonical value, ONE uint64_t (8 bytes), not four Montgomery limbs; roots
+   * and other scalars still pass as uint64_t[4] with the value in [0] and zeros after.  These
+   * fields serve the seven zig-ntt entry points, zntt_field_info / zntt_primitive_root and the
+   * device API (zntt_twiddles_acquire / _release, zntt_ntt_device); bitReverse of 8-byte
+   * elements is zntt_bit_reverse_small.  Batches, coset extensions, polynomial products, the
+   * server, the pipelined host API and the allocation-free entry point take the 256-bit fields
+   * only and reject a small-field table with ZNTT_ERR_UNSUPPORTED_FIELD. */
+  ZNTT_FIELD_GOLDILOCKS = 2,    /* p = 2^64 - 2^32 + 1, two-adicity 32 */
+  ZNTT_FIELD_BABYBEAR = 3       /* p = 15 * 2^27 + 1, two-adicity 27 */
 };
 
 /* One twiddle stage as zig-ntt hands it over: the layout of a Zig
@@ -82,6 +93,8 @@ int zntt_primitive_root(int field, uint32_t log_n, uint64_t root_out[4]);
 
 /* bitReverse(F, data)            libs/ntt/src/root.zig:38-58 */
 int zntt_bit_reverse(uint64_t* data, size_t len);
+/* bitReverse (root.zig:38-58) for 8-byte elements (ZNTT_FIELD_GOLDILOCKS / _BABYBEAR data). */
+int zntt_bit_reverse_small(uint64_t* data, size_t len);
 /* ntt(F, data, log_n, root)       libs/ntt/src/root.zig:65-90 */
 int zntt_ntt(int field, uint64_t* data, size_t len, size_t log_n, const uint64_t root[4]);
 /* intt(F, data, log_n, root)      libs/ntt/src/root.zig:95-107 */

@@ -115,3 +115,42 @@ def test_poly_mul_contract_before_any_device_work(zntt, oracle):
         zntt._check(zntt.lib().zntt_poly_mul(5, None, 0, None, 0, 0, None, None))
     with pytest.raises(zntt.InvalidArgument):
         zntt._check(zntt.lib().zntt_poly_mul(0, None, 2, None, 0, 4, None, None))
+
+
+def test_small_fields_host_side(zntt, oracle):
+    """Goldilocks and BabyBear: field info, primitive roots as zig-field derives them (the
+    roots of the reference's KAT, libs/ntt/src/root.zig:437-447, and the oracle's at every
+    order), and zig-ntt's error order before any device work."""
+    import json
+    import os
+    kats = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ntt_kat.json")))
+    for F, fid in ((zntt.GOLDILOCKS, O.GOLDILOCKS), (zntt.BABYBEAR, O.BABYBEAR)):
+        mod = (ctypes.c_uint64 * 4)()
+        adic = ctypes.c_uint32()
+        assert zntt.lib().zntt_field_info(F.id, mod, ctypes.byref(adic)) == 0
+        assert list(mod) == [F.modulus, 0, 0, 0] and adic.value == F.two_adicity
+        for c in kats:
+            if c["field"] == F.name:
+                assert int(zntt.primitiveRootOfUnity(F, c["log_n"])[0]) == int(c["root"], 16)
+        for log_n in range(F.two_adicity + 1):
+            st, want = O.primitive_root(fid, log_n)
+            assert st == 0
+            got = zntt.primitiveRootOfUnity(F, log_n)
+            assert int(got[0]) == O.to_ints(O.from_mont(fid, want.reshape(1, 4)))[0] and not got[1:].any()
+        with pytest.raises(zntt.OrderTooLarge):
+            zntt.primitiveRootOfUnity(F, F.two_adicity + 1)
+        root = zntt.primitiveRootOfUnity(F, 2)
+        with pytest.raises(zntt.LengthMismatch):
+            zntt.ntt(F, np.zeros(3, dtype=np.uint64), 2, root)
+        with pytest.raises(zntt.LogTooLarge):
+            zntt.intt(F, np.zeros(2, dtype=np.uint64), 64, root)
+        with pytest.raises(zntt.InvalidTwiddles):
+            zntt.nttWithTwiddles(F, np.zeros(4, dtype=np.uint64), 2, [np.zeros(1, dtype=np.uint64)])
+        with pytest.raises(zntt.InvalidLength):
+            zntt.bitReverse(F, np.zeros(3, dtype=np.uint64))
+        # The mirror refuses an array of the 256-bit layout for a small field, and vice versa,
+        # so the library never reads past a buffer.
+        with pytest.raises(zntt.InvalidArgument):
+            zntt.ntt(F, np.zeros((4, 4), dtype=np.uint64), 2, root)
+        with pytest.raises(zntt.InvalidTwiddles):
+            zntt.nttWithTwiddles(zntt.BN254_FR, np.zeros((2, 4), dtype=np.uint64), 1, [np.zeros(1, dtype=np.uint64)])

@@ -256,6 +256,7 @@ def test_device_api_in_and_out_of_place(z, log_n):
             # in place with an explicit scratch, then in place borrowing one
             xi = x.clone()
             s = torch.empty_like(x)
+            torch.cuda.synchronize()  # the clone runs on torch's stream, the library on its own
             z.ntt_device(tw, xi.data_ptr(), xi.data_ptr(), z.FORWARD, d_scratch=s.data_ptr())
             torch.cuda.synchronize()
             np.testing.assert_array_equal(_to_host(xi), want)

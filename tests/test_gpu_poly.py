@@ -102,7 +102,7 @@ def test_poly_mul_device_and_batch_jobs(z):
         st, want, _ = O.poly_mul(fid, a, b, la + lb - 1, workers=WORKERS)
         want = want[:la + lb - 1]
         da, db = _dev(a), _dev(b)
-        out = torch.zeros((la + lb - 1) * 4, dtype=torch.int64, device="cuda")
+        out = torch.empty((la + lb - 1) * 4, dtype=torch.int64, device="cuda")
         z.poly_mul_device(tw(L), da.data_ptr(), la, db.data_ptr(), lb, out.data_ptr())
         torch.cuda.synchronize()
         np.testing.assert_array_equal(_host(out), want, err_msg=f"device {la}x{lb} on 2^{L}")

@@ -40,7 +40,11 @@ def test_noalloc_matches_existing_entry_on_consecutive_calls(z, log_n):
                 x = _vec(z, F, seed, n)
                 want = torch.empty_like(x)
                 z.ntt_device(tw, x.data_ptr(), want.data_ptr(), mode)
+                # The library runs on its own stream and torch on its: order the clone
+                # after the input is made, and the in-place call after the clone.
+                torch.cuda.synchronize()
                 got = x.clone()
+                torch.cuda.synchronize()
                 z.ntt_device_inplace_noalloc(tw, got.data_ptr(), mode)
                 torch.cuda.synchronize()
                 assert torch.equal(got, want), f"{F} 2^{log_n} call {call}"
@@ -51,6 +55,7 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(z):
     F = z.BN254_FR
     with z.DeviceTwiddles(F, 19, z.primitiveRootOfUnity(F, 19)) as tw:
         x = _vec(z, F, 7, 1 << 19)
+        torch.cuda.synchronize()
         before = x.clone()
         with pytest.raises(z.InvalidArgument, match="at most 2\\^18"):
             z.ntt_device_inplace_noalloc(tw, x.data_ptr(), z.FORWARD)

@@ -99,10 +99,12 @@ _ERRORS = {c.code: c for c in (LogTooLarge, LengthMismatch, InvalidTwiddles, Inv
 # --- fields ----------------------------------------------------------------------
 
 class Field:
-    """A scalar field served by the library (the `comptime F` of zig-ntt)."""
+    """A scalar field served by the library (the `comptime F` of zig-ntt).  `limbs` is the
+    element's width in u64 words: 4 Montgomery limbs for the 256-bit fields, 1 canonical
+    value for zig-field's SmallField (Goldilocks, BabyBear)."""
 
-    def __init__(self, fid: int, name: str, modulus: int, two_adicity: int):
-        self.id, self.name, self.modulus, self.two_adicity = fid, name, modulus, two_adicity
+    def __init__(self, fid: int, name: str, modulus: int, two_adicity: int, limbs: int = 4):
+        self.id, self.name, self.modulus, self.two_adicity, self.limbs = fid, name, modulus, two_adicity, limbs
 
     def __repr__(self):
         return f"Field({self.name})"
@@ -111,6 +113,9 @@ class Field:
 BN254_FR = Field(0, "bn254_fr", 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001, 28)
 BLS12_381_FR = Field(1, "bls12_381_fr", 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001, 32)
 FIELDS = (BN254_FR, BLS12_381_FR)
+GOLDILOCKS = Field(2, "goldilocks", 0xFFFFFFFF00000001, 32, limbs=1)
+BABYBEAR = Field(3, "babybear", 0x78000001, 27, limbs=1)
+SMALL_FIELDS = (GOLDILOCKS, BABYBEAR)
 
 FORWARD = 0
 INVERSE = 1
@@ -179,6 +184,7 @@ def lib():
         L.zntt_field_info.argtypes = [i, _U64P, ctypes.POINTER(ctypes.c_uint32)]
         L.zntt_primitive_root.argtypes = [i, ctypes.c_uint32, _U64P]
         L.zntt_bit_reverse.argtypes = [_U64P, sz]
+        L.zntt_bit_reverse_small.argtypes = [_U64P, sz]
         L.zntt_ntt.argtypes = [i, _U64P, sz, sz, _U64P]
         L.zntt_intt.argtypes = [i, _U64P, sz, sz, _U64P]
         L.zntt_precompute_twiddles.argtypes = [i, sz, _U64P, ctypes.POINTER(_U64P)]
@@ -265,7 +271,13 @@ def declared_symbols() -> list[str]:
 
 # --- element helpers ---------------------------------------------------------------
 
-def _p(a: np.ndarray):
+def _p(a: np.ndarray, F: Field | None = None):
+    """The array's data pointer, after checking that its shape is F's element layout:
+    (n, 4) Montgomery limbs, or (n,) canonical values for a small field."""
+    if F is not None and F.limbs == 1:
+        if a.dtype != np.uint64 or not a.flags["C_CONTIGUOUS"] or a.ndim != 1:
+            raise InvalidArgument(f"{F.name} data must be a C-contiguous uint64 array of shape (n,)")
+        return a.ctypes.data_as(_U64P)
     if a.dtype != np.uint64 or not a.flags["C_CONTIGUOUS"] or a.ndim != 2 or a.shape[1] != 4:
         raise InvalidArgument("data must be a C-contiguous uint64 array of shape (n, 4)")
     return a.ctypes.data_as(_U64P)
@@ -293,21 +305,23 @@ def primitiveRootOfUnity(F: Field, log_n: int) -> np.ndarray:
 
 def bitReverse(F: Field, data: np.ndarray) -> None:
     _ensure_init()
-    _check(lib().zntt_bit_reverse(_p(data), len(data)))
+    fn = lib().zntt_bit_reverse_small if F.limbs == 1 else lib().zntt_bit_reverse
+    _check(fn(_p(data, F), len(data)))
 
 
 def ntt(F: Field, data: np.ndarray, log_n: int, root) -> None:
     _ensure_init()
-    _check(lib().zntt_ntt(F.id, _p(data), len(data), log_n, _root(root)))
+    _check(lib().zntt_ntt(F.id, _p(data, F), len(data), log_n, _root(root)))
 
 
 def intt(F: Field, data: np.ndarray, log_n: int, root) -> None:
     _ensure_init()
-    _check(lib().zntt_intt(F.id, _p(data), len(data), log_n, _root(root)))
+    _check(lib().zntt_intt(F.id, _p(data, F), len(data), log_n, _root(root)))
 
 
 class Twiddles(list):
-    """zig-ntt's `[]const []const F`: stage s is an (2^s, 4) uint64 array."""
+    """zig-ntt's `[]const []const F`: stage s is a (2^s, 4) uint64 array (a (2^s,) array for
+    the small fields)."""
 
     def __init__(self, F: Field, stages):
         super().__init__(stages)
@@ -316,9 +330,13 @@ class Twiddles(list):
 
     def stage_array(self):
         arr = (_Stage * max(len(self), 1))()
+        wide = self.field.limbs == 4
         for s, a in enumerate(self):
             if a.dtype != np.uint64 or not a.flags["C_CONTIGUOUS"]:
                 raise InvalidTwiddles("stage arrays must be C-contiguous uint64")
+            if (a.ndim != 2 or a.shape[1] != 4) if wide else a.ndim != 1:
+                raise InvalidTwiddles(f"stage arrays of {self.field.name} must have shape "
+                                      f"{'(len, 4)' if wide else '(len,)'}")
             arr[s].ptr = a.ctypes.data_as(_U64P)
             arr[s].len = len(a)
         return arr
@@ -327,7 +345,7 @@ class Twiddles(list):
 def precomputeTwiddles(F: Field, log_n: int, root) -> Twiddles:
     if log_n >= 64:
         _check(1)
-    stages = [np.zeros((1 << s, 4), dtype=np.uint64) for s in range(log_n)]
+    stages = [np.zeros((1 << s, 4) if F.limbs == 4 else (1 << s,), dtype=np.uint64) for s in range(log_n)]
     ptrs = (_U64P * max(log_n, 1))()
     for s, a in enumerate(stages):
         ptrs[s] = a.ctypes.data_as(_U64P)
@@ -351,13 +369,13 @@ def _as_stages(F: Field, twiddles) -> Twiddles:
 def nttWithTwiddles(F: Field, data: np.ndarray, log_n: int, twiddles) -> None:
     tw = _as_stages(F, twiddles)
     _ensure_init()
-    _check(lib().zntt_ntt_with_twiddles(F.id, _p(data), len(data), log_n, tw.stage_array(), len(tw)))
+    _check(lib().zntt_ntt_with_twiddles(F.id, _p(data, F), len(data), log_n, tw.stage_array(), len(tw)))
 
 
 def inttWithTwiddles(F: Field, data: np.ndarray, log_n: int, twiddles) -> None:
     tw = _as_stages(F, twiddles)
     _ensure_init()
-    _check(lib().zntt_intt_with_twiddles(F.id, _p(data), len(data), log_n, tw.stage_array(), len(tw)))
+    _check(lib().zntt_intt_with_twiddles(F.id, _p(data, F), len(data), log_n, tw.stage_array(), len(tw)))
 
 
 # snake_case aliases

@@ -14,6 +14,7 @@
 #include <cstring>
 
 #include "runtime.hpp"
+#include "small.hpp"
 
 using namespace zntt;
 
@@ -29,6 +30,8 @@ extern "C" int zntt_ntt_host_many(const zntt_twiddles* tw, uint64_t* const* h_da
     if (!h_data[i]) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null vector");
   Context& c = ctx();
   if (c.device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
+  if (is_small_table(tw))
+    return set_error(ZNTT_ERR_UNSUPPORTED_FIELD, "the pipelined host API takes BN254-Fr or BLS12-381-Fr tables only");
   std::lock_guard<std::recursive_mutex> lock(c.mu);
   const TwEntry* e = reinterpret_cast<const TwEntry*>(tw);
   const uint32_t log_n = e->log_n;

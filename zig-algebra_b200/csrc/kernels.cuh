@@ -7,7 +7,9 @@
 namespace zntt {
 
 // Field identifiers shared with the C ABI (include/zntt.h).
-enum FieldId : int { kBn254Fr = 0, kBls12381Fr = 1 };
+// 0 and 1: 256-bit Montgomery fields (32-byte elements, this file's kernels);
+// 2 and 3: SmallField's Goldilocks and BabyBear (8-byte elements, small.cu).
+enum FieldId : int { kBn254Fr = 0, kBls12381Fr = 1, kGoldilocksField = 2, kBabyBearField = 3 };
 
 // One fused radix-2^k pass of the decimation-in-time network.
 //

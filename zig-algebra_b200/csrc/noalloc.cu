@@ -29,6 +29,7 @@
 #include <mutex>
 
 #include "runtime.hpp"
+#include "small.hpp"
 
 namespace zntt {
 
@@ -52,6 +53,8 @@ extern "C" int zntt_ntt_device_inplace_noalloc(const zntt_twiddles* tw, uint64_t
   if (mode != ZNTT_FORWARD && mode != ZNTT_INVERSE) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "unknown mode");
   Context& c = ctx();
   if (c.device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
+  if (is_small_table(tw))
+    return set_error(ZNTT_ERR_UNSUPPORTED_FIELD, "the allocation-free transform takes BN254-Fr or BLS12-381-Fr tables only");
   const TwEntry* e = reinterpret_cast<const TwEntry*>(tw);
   const uint32_t log_n = e->log_n;
   if (log_n > kNoAllocMaxLog)

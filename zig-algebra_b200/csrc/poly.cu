@@ -16,6 +16,7 @@
 
 #include "jobs.hpp"
 #include "runtime.hpp"
+#include "small.hpp"
 
 using namespace zntt;
 
@@ -84,6 +85,8 @@ int zntt_poly_mul_device(const zntt_twiddles* tw, const uint64_t* d_a, size_t le
   if (!tw || !d_a || !d_b || !d_out) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
   Context& c = ctx();
   if (c.device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
+  if (is_small_table(tw))
+    return set_error(ZNTT_ERR_UNSUPPORTED_FIELD, "polynomial products take BN254-Fr or BLS12-381-Fr tables only");
   const TwEntry* e = reinterpret_cast<const TwEntry*>(tw);
   const uint64_t n = 1ull << e->log_n;
   if (len_a < 1 || len_b < 1) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "a factor without coefficients");

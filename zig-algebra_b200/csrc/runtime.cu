@@ -16,6 +16,7 @@
 
 #include "jobs.hpp"
 #include "runtime.hpp"
+#include "small.hpp"
 
 namespace zntt {
 
@@ -430,6 +431,7 @@ void n_inverse(int field, uint32_t log_n, uint64_t* out) {
 static int ntt_with_twiddles_impl(int field, uint64_t* data, size_t len, size_t log_n, const zntt_stage* stages,
                                   size_t num_stages, bool inverse) {
   clear_error();
+  if (is_small_field(field)) return small_ntt_with_twiddles(field, data, len, log_n, stages, num_stages, inverse);
   int rc = check_field(field);
   if (rc) return rc;
   rc = check_shape(len, log_n);
@@ -471,6 +473,7 @@ static int ntt_with_twiddles_impl(int field, uint64_t* data, size_t len, size_t 
 
 static int ntt_root_impl(int field, uint64_t* data, size_t len, size_t log_n, const uint64_t* root, bool inverse) {
   clear_error();
+  if (is_small_field(field)) return small_ntt_root(field, data, len, log_n, root, inverse);
   int rc = check_field(field);
   if (rc) return rc;
   rc = check_shape(len, log_n);
@@ -544,6 +547,7 @@ int zntt_shutdown(void) {
   cudaSetDevice(c.device);
   cudaStreamSynchronize(c.stream);
   while (!c.all_tables.empty()) free_entry(c.all_tables.back());
+  small_shutdown();
   free_coset_tabs();
   c.regs.clear();
   c.pool.trim();
@@ -561,6 +565,7 @@ int zntt_shutdown(void) {
 const char* zntt_last_error(void) { return g_last_error.c_str(); }
 
 int zntt_field_info(int field, uint64_t modulus[4], uint32_t* two_adicity) {
+  if (is_small_field(field)) return small_field_info(field, modulus, two_adicity);
   int rc = check_field(field);
   if (rc) return rc;
   const HostField& F = host_field(field);
@@ -571,6 +576,10 @@ int zntt_field_info(int field, uint64_t modulus[4], uint32_t* two_adicity) {
 
 int zntt_primitive_root(int field, uint32_t log_n, uint64_t root_out[4]) {
   clear_error();
+  if (is_small_field(field)) {
+    if (!root_out) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
+    return small_primitive_root(field, log_n, root_out);
+  }
   int rc = check_field(field);
   if (rc) return rc;
   const HostField& F = host_field(field);
@@ -641,6 +650,7 @@ int zntt_intt(int field, uint64_t* data, size_t len, size_t log_n, const uint64_
 
 int zntt_precompute_twiddles(int field, size_t log_n, const uint64_t root[4], uint64_t* const* stage_out) {
   clear_error();
+  if (is_small_field(field)) return small_precompute(field, log_n, root, stage_out);
   int rc = check_field(field);
   if (rc) return rc;
   if (log_n >= 64) return set_error(ZNTT_ERR_LOG_TOO_LARGE, "log_n >= 64");
@@ -698,6 +708,7 @@ int zntt_precompute_twiddles(int field, size_t log_n, const uint64_t root[4], ui
 }
 
 void zntt_free_twiddles(int field, const zntt_stage* stages, size_t num_stages) {
+  if (is_small_field(field)) return small_free_twiddles(field, stages, num_stages);
   Context& c = ctx();
   std::lock_guard<std::recursive_mutex> lock(c.mu);
   if (!stages || num_stages == 0) return;
@@ -729,6 +740,7 @@ struct zntt_twiddles {};  // opaque: a TwEntry behind the pointer
 
 int zntt_twiddles_acquire(int field, uint32_t log_n, const uint64_t root[4], zntt_twiddles** out) {
   clear_error();
+  if (is_small_field(field)) return small_twiddles_acquire(field, log_n, root, out);
   int rc = check_field(field);
   if (rc) return rc;
   if (!root || !out) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
@@ -747,6 +759,7 @@ int zntt_twiddles_acquire(int field, uint32_t log_n, const uint64_t root[4], znt
 
 int zntt_twiddles_release(zntt_twiddles* tw) {
   if (!tw) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null handle");
+  if (is_small_table(tw)) return small_twiddles_release(tw);
   Context& c = ctx();
   std::lock_guard<std::recursive_mutex> lock(c.mu);
   TwEntry* e = reinterpret_cast<TwEntry*>(tw);
@@ -763,6 +776,7 @@ int zntt_ntt_device(const zntt_twiddles* tw, const uint64_t* d_src, uint64_t* d_
   if (mode != ZNTT_FORWARD && mode != ZNTT_INVERSE) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "unknown mode");
   int rc = check_init();
   if (rc) return rc;
+  if (is_small_table(tw)) return small_ntt_device(tw, d_src, d_dst, d_scratch, mode, stream);
   Context& c = ctx();
   std::lock_guard<std::recursive_mutex> lock(c.mu);
   const TwEntry* e = reinterpret_cast<const TwEntry*>(tw);

@@ -1,0 +1,803 @@
+// small.cu -- zig-ntt over zig-field's SmallField backend: Goldilocks and
+// BabyBear (libs/field/src/field.zig:89-849), the fields of the reference's
+// own known-answer transform tests (libs/ntt/src/root.zig:437-447).
+//
+// An element is SmallField's canonical u64 (8 bytes).  The transform is the
+// same DIT network as the 256-bit path (root.zig:148-212; bit reversal folded
+// into the first pass, tiles of 2^k positions x 2^c neighbouring columns,
+// radix-4 register groups, 1/n fused into the last pass), on 8-byte elements
+// with tiles of 2^12 in shared memory.  Twiddle tables live on the device in
+// twiddle form (small_field.cuh); host tables handed across the C ABI are
+// canonical, in zig-ntt's layout.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "runtime.hpp"
+#include "small.hpp"
+#include "small_field.cuh"
+
+namespace zntt {
+
+namespace {
+
+// ---- host arithmetic ----------------------------------------------------------
+
+struct SmallHost {
+  int field;
+  uint64_t p;
+  uint32_t two_adicity;
+  uint64_t r;  // R mod p: the twiddle-form factor (1 for Goldilocks, 2^32 for BabyBear)
+
+  uint64_t mul(uint64_t a, uint64_t b) const { return (uint64_t)((unsigned __int128)a * b % p); }
+  uint64_t pow(uint64_t a, uint64_t e) const {
+    uint64_t r1 = 1 % p;
+    while (e) {
+      if (e & 1) r1 = mul(r1, a);
+      a = mul(a, a);
+      e >>= 1;
+    }
+    return r1;
+  }
+  uint64_t inv(uint64_t a) const { return pow(a, p - 2); }  // p prime; inv(0) = 0
+  uint64_t to_tw(uint64_t w) const { return mul(w % p, r); }
+  uint64_t from_tw(uint64_t w) const { return mul(w, inv(r)); }
+};
+
+const SmallHost kGoldilocksHost{kGoldilocksField, Goldilocks::P, 32, 1};
+const SmallHost kBabyBearHost{kBabyBearField, BabyBear::P, 27, (uint64_t)(((unsigned __int128)1 << 32) % BabyBear::P)};
+
+const SmallHost& small_host(int field) { return field == kGoldilocksField ? kGoldilocksHost : kBabyBearHost; }
+
+// ---- kernels -------------------------------------------------------------------
+
+constexpr int kSmallLogTile = 12;
+constexpr int kSmallThreads = 256;
+constexpr uint32_t kSmallKmax = 10;  // keeps 2^(12 - k) >= 4 columns (32-byte rows) per tile row
+
+struct SmallPass {
+  const uint64_t* src;
+  uint64_t* dst;
+  const uint64_t* tw;  // twiddle form, stage s at entry 2^s - 1
+  uint32_t log_n, S, k, c, first, inverse, tw0_one, scale;
+  uint64_t scale_val;  // twiddle form
+};
+
+__device__ __forceinline__ uint32_t rev_bits_small(uint32_t x, uint32_t bits) {
+  return bits == 0 ? 0u : (__brev(x) >> (32 - bits));
+}
+
+// Twiddle of global stage s for butterfly jg: forward tw[s-1][jg], inverse 1
+// (jg = 0) or -tw[s-1][2^(s-1) - jg] (root.zig:199); false when it is one.
+template <class SF>
+__device__ __forceinline__ bool small_twiddle(const SmallPass& pp, const uint64_t* stw, uint64_t half, uint64_t jg,
+                                              uint64_t& w) {
+  if (jg == 0 && (pp.inverse | pp.tw0_one)) return false;
+  w = pp.inverse ? SF::neg(__ldg(stw + (half - jg))) : __ldg(stw + jg);
+  return true;
+}
+
+template <class SF>
+__device__ __forceinline__ void small_butterfly(uint64_t& u, uint64_t& v, bool mul, uint64_t w) {
+  const uint64_t t = mul ? SF::mul(w, v) : v;
+  v = SF::sub(u, t);
+  u = SF::add(u, t);
+}
+
+template <class SF, int LOG_TILE, int THREADS>
+__global__ void __launch_bounds__(THREADS) small_pass_kernel(SmallPass pp) {
+  constexpr uint32_t TILE_MAX = 1u << LOG_TILE;
+  __shared__ uint64_t sm[TILE_MAX];
+  const uint32_t k = pp.k, c = pp.c, C = 1u << c;
+  const uint32_t tile = 1u << (k + c);
+  const uint32_t tid = threadIdx.x;
+  const uint64_t blk = blockIdx.x;
+  uint64_t hi_base = 0, m0 = 0, col0 = 0;
+  if (pp.first) {
+    col0 = blk << c;
+  } else {
+    const uint32_t mlog = pp.S - c;
+    hi_base = (blk >> mlog) << (pp.S + k);
+    m0 = (blk & ((1ull << mlog) - 1)) << c;
+  }
+  const uint32_t xcols_log = pp.log_n - k;
+
+#pragma unroll
+  for (uint32_t q = 0; q < TILE_MAX / THREADS; q++) {
+    const uint32_t e = tid + q * THREADS;
+    if (e < tile) {
+      const uint32_t col = e & (C - 1), row = e >> c;
+      uint64_t g;
+      uint32_t t;
+      if (pp.first) {
+        g = ((uint64_t)row << xcols_log) + col0 + col;
+        t = rev_bits_small(row, k);
+      } else {
+        g = hi_base + ((uint64_t)row << pp.S) + m0 + col;
+        t = row;
+      }
+      sm[(t << c) | col] = pp.src[g];
+    }
+  }
+  __syncthreads();
+
+  uint32_t i = 1;
+  if (k & 1) {
+    const uint64_t half = 1ull << pp.S;
+    const uint64_t* stw = pp.tw + (half - 1);
+#pragma unroll
+    for (uint32_t q = 0; q < TILE_MAX / 2 / THREADS; q++) {
+      const uint32_t b = tid + q * THREADS;
+      if (b < tile / 2) {
+        const uint32_t col = b & (C - 1), t0 = (b >> c) << 1;
+        const uint64_t jg = pp.first ? 0 : m0 + col;
+        const uint32_t e0 = (t0 << c) | col, e1 = e0 + C;
+        uint64_t u = sm[e0], v = sm[e1], w = 0;
+        const bool mul = small_twiddle<SF>(pp, stw, half, jg, w);
+        small_butterfly<SF>(u, v, mul, w);
+        sm[e0] = u;
+        sm[e1] = v;
+      }
+    }
+    __syncthreads();
+    i = 2;
+  }
+  for (; i < k; i += 2) {
+    const uint32_t h = 1u << (i - 1);
+    const uint64_t half1 = 1ull << (pp.S + i - 1), half2 = half1 << 1;
+    const uint64_t* stw1 = pp.tw + (half1 - 1);
+    const uint64_t* stw2 = pp.tw + (half2 - 1);
+#pragma unroll
+    for (uint32_t q = 0; q < TILE_MAX / 4 / THREADS; q++) {
+      const uint32_t ga = tid + q * THREADS;
+      if (ga < tile / 4) {
+        const uint32_t col = ga & (C - 1), g = ga >> c;
+        const uint32_t j = g & (h - 1);
+        const uint32_t t0 = ((g >> (i - 1)) << (i + 1)) | j;
+        const uint32_t e0 = (t0 << c) | col, eh = h << c;
+        uint64_t jg1, jg3;
+        if (pp.first) {
+          jg1 = j;
+          jg3 = j + h;
+        } else {
+          jg1 = ((uint64_t)j << pp.S) + m0 + col;
+          jg3 = jg1 + ((uint64_t)h << pp.S);
+        }
+        uint64_t w1 = 0, w2 = 0, w3 = 0;
+        const bool m1 = small_twiddle<SF>(pp, stw1, half1, jg1, w1);
+        const bool m2 = small_twiddle<SF>(pp, stw2, half2, jg1, w2);
+        const bool m3 = small_twiddle<SF>(pp, stw2, half2, jg3, w3);
+        uint64_t x0 = sm[e0], x1 = sm[e0 + eh], x2 = sm[e0 + 2 * eh], x3 = sm[e0 + 3 * eh];
+        small_butterfly<SF>(x0, x1, m1, w1);
+        small_butterfly<SF>(x2, x3, m1, w1);
+        small_butterfly<SF>(x0, x2, m2, w2);
+        small_butterfly<SF>(x1, x3, m3, w3);
+        sm[e0] = x0;
+        sm[e0 + eh] = x1;
+        sm[e0 + 2 * eh] = x2;
+        sm[e0 + 3 * eh] = x3;
+      }
+    }
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (uint32_t q = 0; q < TILE_MAX / THREADS; q++) {
+    const uint32_t e = tid + q * THREADS;
+    if (e < tile) {
+      const uint32_t col = e & (C - 1), row = e >> c;
+      const uint64_t g = pp.first ? ((uint64_t)rev_bits_small((uint32_t)(col0 + col), xcols_log) << k) + row
+                                  : hi_base + ((uint64_t)row << pp.S) + m0 + col;
+      uint64_t x = sm[(row << c) | col];
+      if (pp.scale) x = SF::mul(pp.scale_val, x);
+      pp.dst[g] = x;
+    }
+  }
+}
+
+// Flat table entry e = 2^s - 1 + j holds root^(j * 2^(log_n - 1 - s)), in
+// twiddle form, from three power tables pw[t][i] = root^(i * 1024^t).
+template <class SF>
+__global__ void small_twiddle_kernel(const uint64_t* __restrict__ pw, uint64_t* __restrict__ out, uint32_t log_n) {
+  const uint64_t total = (1ull << log_n) - 1;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < total;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t s = 63 - __clzll(e + 1);
+    const uint64_t j = e + 1 - (1ull << s);
+    const uint64_t x = j << (log_n - 1 - s);
+    uint64_t v = SF::mul(__ldg(pw + (x & 1023)), __ldg(pw + 1024 + ((x >> 10) & 1023)));
+    out[e] = SF::mul(v, __ldg(pw + 2048 + (x >> 20)));
+  }
+}
+
+// out[i] = in[i] * f (twiddle form in, f chosen by the caller): converts
+// between canonical and twiddle form (f = R^2 mod p, or canonical 1).
+template <class SF>
+__global__ void small_scale_kernel(const uint64_t* __restrict__ in, uint64_t* __restrict__ out, uint64_t count,
+                                   uint64_t f) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = SF::mul(f, __ldg(in + i));
+}
+
+__global__ void small_bit_reverse_kernel(const uint64_t* __restrict__ src, uint64_t* __restrict__ dst,
+                                         uint32_t log_n) {
+  const uint64_t n = 1ull << log_n;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    dst[__brevll(i) >> (64 - log_n)] = src[i];
+}
+
+int grid_for(uint64_t count) { return (int)std::min<uint64_t>((count + 255) / 256, 148 * 16); }
+
+cudaError_t launch_small_pass(int field, const SmallPass& pp, uint64_t tiles, cudaStream_t st) {
+  if (field == kGoldilocksField)
+    small_pass_kernel<Goldilocks, kSmallLogTile, kSmallThreads><<<(unsigned)tiles, kSmallThreads, 0, st>>>(pp);
+  else
+    small_pass_kernel<BabyBear, kSmallLogTile, kSmallThreads><<<(unsigned)tiles, kSmallThreads, 0, st>>>(pp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_small_scale(int field, const uint64_t* in, uint64_t* out, uint64_t count, uint64_t f,
+                               cudaStream_t st) {
+  if (count == 0) return cudaSuccess;
+  if (field == kGoldilocksField)
+    small_scale_kernel<Goldilocks><<<grid_for(count), 256, 0, st>>>(in, out, count, f);
+  else
+    small_scale_kernel<BabyBear><<<grid_for(count), 256, 0, st>>>(in, out, count, f);
+  return cudaGetLastError();
+}
+
+// ---- plans ---------------------------------------------------------------------
+
+struct SmallPlanPass {
+  uint32_t S, k, c;
+};
+
+std::vector<SmallPlanPass> small_plan(uint32_t log_n) {
+  std::vector<SmallPlanPass> plan;
+  const uint32_t lt = kSmallLogTile;
+  if (log_n == 0) return plan;
+  if (log_n <= lt) {
+    plan.push_back({0, log_n, 0});
+    return plan;
+  }
+  const uint32_t P = (log_n + kSmallKmax - 1) / kSmallKmax;
+  uint32_t S = 0;
+  for (uint32_t p = 0; p < P; p++) {
+    const uint32_t k = log_n / P + (p < log_n % P ? 1 : 0);
+    uint32_t c = lt - k;
+    const uint32_t lim = p == 0 ? log_n - k : S;
+    if (c > lim) c = lim;
+    plan.push_back({S, k, c});
+    S += k;
+  }
+  return plan;
+}
+
+// ---- tables ----------------------------------------------------------------------
+
+// A device table.  The leading members match TwEntry's (field, log_n), so the
+// 256-bit entry points recognise a small-field handle by its field and refuse it.
+struct SmallTable {
+  int field = 0;
+  uint32_t log_n = 0;
+  uint64_t root = 0;          // canonical; the key of root-derived tables
+  uint64_t* d_table = nullptr;  // 2^log_n - 1 entries in twiddle form (one when log_n == 0)
+  size_t bytes = 0;
+  int refs = 0;
+  bool tw0_one = true;
+  bool foreign = false;
+  uint64_t last_use = 0;
+};
+
+struct SmallRegistration {
+  int field = 0;
+  uint32_t log_n = 0;
+  std::vector<const uint64_t*> stage_ptrs;
+  std::vector<uint64_t> probe;  // entries 0 and 1 of each stage (when present)
+  SmallTable* entry = nullptr;
+};
+
+struct SmallState {
+  std::map<std::string, SmallTable*> by_key;
+  std::vector<SmallTable*> all;
+  std::vector<SmallRegistration> regs;
+  uint64_t clock = 0;
+  size_t idle_budget = (size_t)4 << 30;  // idle root-derived tables kept up to this
+};
+
+SmallState& small_state() {
+  static SmallState s;
+  return s;
+}
+
+std::string small_key(int field, uint32_t log_n, uint64_t root) {
+  return std::to_string(field) + ":" + std::to_string(log_n) + ":" + std::to_string(root);
+}
+
+size_t small_entries(uint32_t log_n) { return log_n == 0 ? 1 : ((size_t)1 << log_n) - 1; }
+
+void small_free_entry(SmallTable* e) {
+  SmallState& s = small_state();
+  if (e->d_table) cudaFree(e->d_table);
+  s.all.erase(std::remove(s.all.begin(), s.all.end(), e), s.all.end());
+  for (auto it = s.by_key.begin(); it != s.by_key.end(); ++it)
+    if (it->second == e) {
+      s.by_key.erase(it);
+      break;
+    }
+  delete e;
+}
+
+// Frees idle root-derived tables, oldest first, until the idle ones (plus
+// `need` bytes about to be allocated) fit the budget.
+void small_evict(size_t need) {
+  SmallState& s = small_state();
+  for (;;) {
+    size_t idle = 0;
+    SmallTable* oldest = nullptr;
+    for (SmallTable* e : s.all)
+      if (e->refs == 0) {
+        idle += e->bytes;
+        if (!oldest || e->last_use < oldest->last_use) oldest = e;
+      }
+    if (!oldest || idle + need <= s.idle_budget) return;
+    small_free_entry(oldest);
+  }
+}
+
+// A caller's table is freed with its last user; a root-derived one stays
+// cached while idle tables fit the budget.
+void small_release(SmallTable* e) {
+  if (!e) return;
+  if (--e->refs <= 0) {
+    e->refs = 0;
+    if (e->foreign) small_free_entry(e);
+    else small_evict(0);
+  }
+}
+
+int small_acquire(int field, uint32_t log_n, uint64_t root, SmallTable** out) {
+  Context& c = ctx();
+  SmallState& s = small_state();
+  const std::string key = small_key(field, log_n, root);
+  auto it = s.by_key.find(key);
+  if (it != s.by_key.end()) {
+    it->second->refs++;
+    it->second->last_use = ++s.clock;
+    *out = it->second;
+    return ZNTT_OK;
+  }
+  const SmallHost& H = small_host(field);
+  SmallTable* e = new SmallTable();
+  e->field = field;
+  e->log_n = log_n;
+  e->root = root;
+  e->bytes = small_entries(log_n) * 8;
+  small_evict(e->bytes);
+  cudaError_t ce = cudaMalloc((void**)&e->d_table, e->bytes);
+  if (ce != cudaSuccess) {
+    delete e;
+    return cuda_fail(ce, "twiddle table");
+  }
+  if (log_n > 0) {
+    // pw[t][i] = root^(i * 1024^t), computed canonically, stored in twiddle form.
+    std::vector<uint64_t> pw(3 * 1024);
+    uint64_t step = root;
+    for (int t = 0; t < 3; t++) {
+      uint64_t cur = 1;
+      for (int i = 0; i < 1024; i++) {
+        pw[t * 1024 + i] = H.to_tw(cur);
+        cur = H.mul(cur, step);
+      }
+      step = H.pow(step, 1024);
+    }
+    void* d_pw = nullptr;
+    int rc = pool_get(pw.size() * 8, &d_pw);
+    if (rc) {
+      cudaFree(e->d_table);
+      delete e;
+      return rc;
+    }
+    ce = cudaMemcpyAsync(d_pw, pw.data(), pw.size() * 8, cudaMemcpyHostToDevice, c.stream);
+    const uint64_t total = small_entries(log_n);
+    if (ce == cudaSuccess) {
+      if (field == kGoldilocksField)
+        small_twiddle_kernel<Goldilocks><<<grid_for(total), 256, 0, c.stream>>>((const uint64_t*)d_pw, e->d_table,
+                                                                                 log_n);
+      else
+        small_twiddle_kernel<BabyBear><<<grid_for(total), 256, 0, c.stream>>>((const uint64_t*)d_pw, e->d_table,
+                                                                               log_n);
+      ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(c.stream);
+    pool_put(d_pw, pw.size() * 8);
+    if (ce != cudaSuccess) {
+      cudaFree(e->d_table);
+      delete e;
+      return cuda_fail(ce, "twiddle table");
+    }
+  }
+  e->refs = 1;
+  e->last_use = ++s.clock;
+  s.all.push_back(e);
+  s.by_key[key] = e;
+  *out = e;
+  return ZNTT_OK;
+}
+
+// A caller's canonical host table, converted to twiddle form on the device.
+int small_upload_foreign(int field, uint32_t log_n, const zntt_stage* stages, SmallTable** out) {
+  Context& c = ctx();
+  const SmallHost& H = small_host(field);
+  SmallTable* e = new SmallTable();
+  e->field = field;
+  e->log_n = log_n;
+  e->foreign = true;
+  e->bytes = small_entries(log_n) * 8;
+  cudaError_t ce = cudaMalloc((void**)&e->d_table, e->bytes);
+  if (ce != cudaSuccess) {
+    delete e;
+    return cuda_fail(ce, "foreign twiddle table");
+  }
+  for (uint32_t s = 0; s < log_n && ce == cudaSuccess; s++) {
+    if (stages[s].ptr[0] != 1) e->tw0_one = false;
+    ce = cudaMemcpyAsync(e->d_table + (((size_t)1 << s) - 1), stages[s].ptr, ((size_t)1 << s) * 8,
+                         cudaMemcpyHostToDevice, c.stream);
+  }
+  // Canonical -> twiddle form: mul(x, R^2) = x * R.  Entries at or above p are
+  // reduced on the way (the reference's Fields are canonical already).
+  if (ce == cudaSuccess)
+    ce = launch_small_scale(field, e->d_table, e->d_table, small_entries(log_n) - (log_n == 0 ? 1 : 0),
+                            H.mul(H.r, H.r), c.stream);
+  if (ce != cudaSuccess) {
+    cudaStreamSynchronize(c.stream);
+    cudaFree(e->d_table);
+    delete e;
+    return cuda_fail(ce, "foreign twiddle upload");
+  }
+  e->refs = 1;
+  small_state().all.push_back(e);
+  *out = e;
+  return ZNTT_OK;
+}
+
+SmallRegistration* small_find_registration(int field, uint32_t log_n, const zntt_stage* stages) {
+  for (SmallRegistration& r : small_state().regs) {
+    if (r.field != field || r.log_n != log_n) continue;
+    bool same = true;
+    for (uint32_t s = 0; s < log_n && same; s++) same = r.stage_ptrs[s] == stages[s].ptr;
+    for (uint32_t s = 0; s < log_n && same; s++) {
+      const size_t m = std::min<size_t>((size_t)1 << s, 2);
+      same = std::memcmp(stages[s].ptr, &r.probe[2 * s], m * 8) == 0;
+    }
+    if (same) return &r;
+  }
+  return nullptr;
+}
+
+// ---- transforms ----------------------------------------------------------------
+
+// src -> dst over 2^log_n device elements; scratch (2^log_n) is needed when
+// src == dst and there are several passes.
+int small_run(const SmallTable* t, const uint64_t* src, uint64_t* dst, uint64_t* scratch, bool inverse, bool scale,
+              uint64_t scale_tw, cudaStream_t st) {
+  const std::vector<SmallPlanPass> plan = small_plan(t->log_n);
+  if (plan.empty()) {  // one element: a copy (the 1/n scale is by one)
+    if (src != dst) {
+      cudaError_t ce = cudaMemcpyAsync(dst, src, 8, cudaMemcpyDeviceToDevice, st);
+      if (ce != cudaSuccess) return cuda_fail(ce, "copy");
+    }
+    return ZNTT_OK;
+  }
+  uint64_t* mid = (src == dst && plan.size() > 1) ? scratch : dst;
+  for (size_t p = 0; p < plan.size(); p++) {
+    const bool first = p == 0, last = p + 1 == plan.size();
+    SmallPass pp;
+    std::memset(&pp, 0, sizeof(pp));
+    pp.src = first ? src : mid;
+    pp.dst = last ? dst : mid;
+    pp.tw = t->d_table;
+    pp.log_n = t->log_n;
+    pp.S = plan[p].S;
+    pp.k = plan[p].k;
+    pp.c = plan[p].c;
+    pp.first = first;
+    pp.inverse = inverse;
+    pp.tw0_one = t->tw0_one;
+    pp.scale = last && scale;
+    pp.scale_val = scale_tw;
+    const uint64_t tiles = (1ull << t->log_n) >> (pp.k + pp.c);
+    cudaError_t ce = launch_small_pass(t->field, pp, tiles, st);
+    if (ce != cudaSuccess) return cuda_fail(ce, "small-field pass");
+  }
+  return ZNTT_OK;
+}
+
+int small_transform_host(const SmallTable* t, uint64_t* data, bool inverse, bool scale, uint64_t scale_tw) {
+  Context& c = ctx();
+  const size_t bytes = ((size_t)8) << t->log_n;
+  void* a = nullptr;
+  void* b = nullptr;
+  int rc = pool_get(bytes, &a);
+  if (!rc) rc = pool_get(bytes, &b);
+  cudaError_t ce = cudaSuccess;
+  if (!rc) {
+    ce = cudaMemcpyAsync(a, data, bytes, cudaMemcpyHostToDevice, c.stream);
+    if (ce == cudaSuccess) rc = small_run(t, (const uint64_t*)a, (uint64_t*)b, nullptr, inverse, scale, scale_tw, c.stream);
+    if (ce == cudaSuccess && !rc) ce = cudaMemcpyAsync(data, b, bytes, cudaMemcpyDeviceToHost, c.stream);
+    cudaError_t ce2 = cudaStreamSynchronize(c.stream);
+    if (ce == cudaSuccess) ce = ce2;
+    if (ce != cudaSuccess && !rc) rc = cuda_fail(ce, "small-field transform");
+  }
+  if (a) pool_put(a, bytes);
+  if (b) pool_put(b, bytes);
+  return rc;
+}
+
+uint64_t n_inverse_tw(const SmallHost& H, uint32_t log_n) { return H.to_tw(H.inv(((uint64_t)1 << log_n) % H.p)); }
+
+int check_small_shape(size_t len, size_t log_n) {
+  if (log_n >= 64) return set_error(ZNTT_ERR_LOG_TOO_LARGE, "log_n >= 64");
+  if (len != ((size_t)1 << log_n)) return set_error(ZNTT_ERR_LENGTH_MISMATCH, "data.len != 2^log_n");
+  return ZNTT_OK;
+}
+
+int check_small_ready(size_t log_n) {
+  if (log_n > 31) return set_error(ZNTT_ERR_OUT_OF_MEMORY, "transform larger than 2^31 elements");
+  if (ctx().device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
+  return ZNTT_OK;
+}
+
+}  // namespace
+
+bool is_small_field(int field) { return field == kGoldilocksField || field == kBabyBearField; }
+
+bool is_small_table(const void* handle) {
+  return handle && is_small_field(*static_cast<const int*>(handle));
+}
+
+int small_field_info(int field, uint64_t* modulus, uint32_t* two_adicity) {
+  const SmallHost& H = small_host(field);
+  if (modulus) {
+    modulus[0] = H.p;
+    modulus[1] = modulus[2] = modulus[3] = 0;
+  }
+  if (two_adicity) *two_adicity = H.two_adicity;
+  return ZNTT_OK;
+}
+
+// roots.zig:22-30, 149-158: z = the first quadratic non-residue from 2, and
+// the root of order 2^log_n is z^(odd_part << (two_adicity - log_n)) =
+// z^((p - 1) >> log_n).
+int small_primitive_root(int field, uint32_t log_n, uint64_t* root_out) {
+  const SmallHost& H = small_host(field);
+  if (log_n > H.two_adicity) return set_error(ZNTT_ERR_ORDER_TOO_LARGE, "log_n exceeds the two-adicity");
+  uint64_t z = 2;
+  while (H.pow(z, (H.p - 1) / 2) != H.p - 1) z++;
+  root_out[0] = H.pow(z, (H.p - 1) >> log_n);
+  root_out[1] = root_out[2] = root_out[3] = 0;
+  return ZNTT_OK;
+}
+
+int small_bit_reverse(uint64_t* data, size_t len) {
+  if (len == 0 || (len & (len - 1)) != 0) return set_error(ZNTT_ERR_INVALID_LENGTH, "length is 0 or not 2^k");
+  if (!data) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null data");
+  const uint32_t log_n = (uint32_t)__builtin_ctzll(len);
+  int rc = check_small_ready(log_n);
+  if (rc) return rc;
+  if (len == 1) return ZNTT_OK;
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  void* a = nullptr;
+  void* b = nullptr;
+  rc = pool_get(len * 8, &a);
+  if (!rc) rc = pool_get(len * 8, &b);
+  cudaError_t ce = cudaSuccess;
+  if (!rc) {
+    ce = cudaMemcpyAsync(a, data, len * 8, cudaMemcpyHostToDevice, c.stream);
+    if (ce == cudaSuccess) {
+      small_bit_reverse_kernel<<<grid_for(len), 256, 0, c.stream>>>((const uint64_t*)a, (uint64_t*)b, log_n);
+      ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(data, b, len * 8, cudaMemcpyDeviceToHost, c.stream);
+    cudaError_t ce2 = cudaStreamSynchronize(c.stream);
+    if (ce == cudaSuccess) ce = ce2;
+    if (ce != cudaSuccess) rc = cuda_fail(ce, "bit reverse");
+  }
+  if (a) pool_put(a, len * 8);
+  if (b) pool_put(b, len * 8);
+  return rc;
+}
+
+int small_ntt_root(int field, uint64_t* data, size_t len, size_t log_n, const uint64_t* root, bool inverse) {
+  int rc = check_small_shape(len, log_n);
+  if (rc) return rc;
+  if (!data || !root) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
+  rc = check_small_ready(log_n);
+  if (rc) return rc;
+  if (log_n == 0) return ZNTT_OK;
+  const SmallHost& H = small_host(field);
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  // intt(root) is ntt(root.inv()) followed by the 1/n scale (root.zig:100-106).
+  const uint64_t r = inverse ? H.inv(root[0] % H.p) : root[0] % H.p;
+  SmallTable* t = nullptr;
+  rc = small_acquire(field, (uint32_t)log_n, r, &t);
+  if (rc) return rc;
+  rc = small_transform_host(t, data, false, inverse, n_inverse_tw(H, (uint32_t)log_n));
+  small_release(t);
+  return rc;
+}
+
+int small_precompute(int field, size_t log_n, const uint64_t* root, uint64_t* const* stage_out) {
+  if (log_n >= 64) return set_error(ZNTT_ERR_LOG_TOO_LARGE, "log_n >= 64");
+  if (log_n > 31) return set_error(ZNTT_ERR_OUT_OF_MEMORY, "transform larger than 2^31 elements");
+  if (log_n == 0) return ZNTT_OK;
+  if (!root || !stage_out) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
+  for (size_t s = 0; s < log_n; s++)
+    if (!stage_out[s]) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null stage pointer");
+  int rc = check_small_ready(log_n);
+  if (rc) return rc;
+  const SmallHost& H = small_host(field);
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  SmallTable* t = nullptr;
+  rc = small_acquire(field, (uint32_t)log_n, root[0] % H.p, &t);
+  if (rc) return rc;
+  // Twiddle form -> canonical (mul by canonical one), then download by stage.
+  const size_t entries = small_entries((uint32_t)log_n);
+  void* canon = nullptr;
+  rc = pool_get(entries * 8, &canon);
+  if (rc) {
+    small_release(t);
+    return rc;
+  }
+  cudaError_t ce = launch_small_scale(field, t->d_table, (uint64_t*)canon, entries, 1, c.stream);
+  for (size_t s = 0; s < log_n && ce == cudaSuccess; s++)
+    ce = cudaMemcpyAsync(stage_out[s], (uint64_t*)canon + (((size_t)1 << s) - 1), ((size_t)1 << s) * 8,
+                         cudaMemcpyDeviceToHost, c.stream);
+  cudaError_t ce2 = cudaStreamSynchronize(c.stream);
+  pool_put(canon, entries * 8);
+  if (ce == cudaSuccess) ce = ce2;
+  if (ce != cudaSuccess) {
+    small_release(t);
+    return cuda_fail(ce, "twiddle download");
+  }
+  SmallState& st = small_state();
+  for (auto it = st.regs.begin(); it != st.regs.end();) {
+    bool same = it->field == field && it->log_n == log_n;
+    for (size_t s = 0; s < log_n && same; s++) same = it->stage_ptrs[s] == stage_out[s];
+    if (same) {
+      small_release(it->entry);
+      it = st.regs.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  SmallRegistration r;
+  r.field = field;
+  r.log_n = (uint32_t)log_n;
+  r.entry = t;
+  r.probe.assign(2 * log_n, 0);
+  for (size_t s = 0; s < log_n; s++) {
+    r.stage_ptrs.push_back(stage_out[s]);
+    const size_t m = std::min<size_t>((size_t)1 << s, 2);
+    std::memcpy(&r.probe[2 * s], stage_out[s], m * 8);
+  }
+  st.regs.push_back(std::move(r));
+  return ZNTT_OK;
+}
+
+void small_free_twiddles(int field, const zntt_stage* stages, size_t num_stages) {
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  if (!stages || num_stages == 0) return;
+  SmallState& st = small_state();
+  for (auto it = st.regs.begin(); it != st.regs.end(); ++it) {
+    if (it->field != field || it->log_n != num_stages) continue;
+    bool same = true;
+    for (size_t s = 0; s < num_stages && same; s++) same = it->stage_ptrs[s] == stages[s].ptr;
+    if (same) {
+      small_release(it->entry);
+      st.regs.erase(it);
+      return;
+    }
+  }
+}
+
+int small_ntt_with_twiddles(int field, uint64_t* data, size_t len, size_t log_n, const zntt_stage* stages,
+                            size_t num_stages, bool inverse) {
+  int rc = check_small_shape(len, log_n);
+  if (rc) return rc;
+  if (num_stages != log_n) return set_error(ZNTT_ERR_INVALID_TWIDDLES, "twiddles.len != log_n");
+  if (num_stages && !stages) return set_error(ZNTT_ERR_INVALID_TWIDDLES, "null twiddle table");
+  for (size_t s = 0; s < num_stages; s++)
+    if (stages[s].len != ((size_t)1 << s) || !stages[s].ptr)
+      return set_error(ZNTT_ERR_INVALID_TWIDDLES, "twiddle stage " + std::to_string(s) + " has the wrong length");
+  if (!data) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null data");
+  rc = check_small_ready(log_n);
+  if (rc) return rc;
+  if (log_n == 0) return ZNTT_OK;
+  const SmallHost& H = small_host(field);
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  SmallTable* t = nullptr;
+  bool foreign = false;
+  SmallRegistration* reg = small_find_registration(field, (uint32_t)log_n, stages);
+  if (reg) {
+    t = reg->entry;
+  } else {
+    rc = small_upload_foreign(field, (uint32_t)log_n, stages, &t);
+    if (rc) return rc;
+    foreign = true;
+  }
+  rc = small_transform_host(t, data, inverse, inverse, n_inverse_tw(H, (uint32_t)log_n));
+  if (foreign) small_release(t);
+  return rc;
+}
+
+int small_twiddles_acquire(int field, uint32_t log_n, const uint64_t* root, zntt_twiddles** out) {
+  if (!root || !out) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
+  int rc = check_small_ready(log_n);
+  if (rc) return rc;
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  SmallTable* t = nullptr;
+  rc = small_acquire(field, log_n, root[0] % small_host(field).p, &t);
+  if (rc) return rc;
+  *out = reinterpret_cast<zntt_twiddles*>(t);
+  return ZNTT_OK;
+}
+
+int small_twiddles_release(zntt_twiddles* tw) {
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  SmallTable* t = reinterpret_cast<SmallTable*>(tw);
+  SmallState& s = small_state();
+  if (std::find(s.all.begin(), s.all.end(), t) == s.all.end())
+    return set_error(ZNTT_ERR_INVALID_ARGUMENT, "unknown twiddle handle");
+  small_release(t);
+  return ZNTT_OK;
+}
+
+int small_ntt_device(const zntt_twiddles* tw, const uint64_t* d_src, uint64_t* d_dst, uint64_t* d_scratch, int mode,
+                     void* stream) {
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  const SmallTable* t = reinterpret_cast<const SmallTable*>(tw);
+  const SmallHost& H = small_host(t->field);
+  const bool inverse = mode == ZNTT_INVERSE;
+  const uint64_t ninv = n_inverse_tw(H, t->log_n);
+  cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+  const bool need_scratch = d_src == d_dst && small_plan(t->log_n).size() > 1;
+  if (need_scratch && !d_scratch) {
+    const size_t bytes = ((size_t)8) << t->log_n;
+    void* s = nullptr;
+    int rc = pool_get(bytes, &s);
+    if (rc) return rc;
+    rc = small_run(t, d_src, d_dst, (uint64_t*)s, inverse, inverse, ninv, st);
+    cudaError_t ce = cudaStreamSynchronize(st);
+    pool_put(s, bytes);
+    if (rc) return rc;
+    if (ce != cudaSuccess) return cuda_fail(ce, "transform");
+    return ZNTT_OK;
+  }
+  return small_run(t, d_src, d_dst, d_scratch, inverse, inverse, ninv, st);
+}
+
+void small_shutdown() {
+  SmallState& s = small_state();
+  while (!s.all.empty()) small_free_entry(s.all.back());
+  s.regs.clear();
+}
+
+}  // namespace zntt
+
+extern "C" int zntt_bit_reverse_small(uint64_t* data, size_t len) {
+  zntt::clear_error();
+  return zntt::small_bit_reverse(data, len);
+}

@@ -1,0 +1,31 @@
+// small.hpp -- the SmallField (Goldilocks, BabyBear) path of the C ABI
+// (small.cu), dispatched to by the entry points of runtime.cu when the field
+// id or twiddle handle is a small field's.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "zntt.h"
+
+namespace zntt {
+
+bool is_small_field(int field);
+// A twiddle handle made for a small field (its leading field id says so).
+bool is_small_table(const void* handle);
+
+int small_field_info(int field, uint64_t* modulus, uint32_t* two_adicity);
+int small_primitive_root(int field, uint32_t log_n, uint64_t* root_out);
+int small_bit_reverse(uint64_t* data, size_t len);
+int small_ntt_root(int field, uint64_t* data, size_t len, size_t log_n, const uint64_t* root, bool inverse);
+int small_precompute(int field, size_t log_n, const uint64_t* root, uint64_t* const* stage_out);
+void small_free_twiddles(int field, const zntt_stage* stages, size_t num_stages);
+int small_ntt_with_twiddles(int field, uint64_t* data, size_t len, size_t log_n, const zntt_stage* stages,
+                            size_t num_stages, bool inverse);
+int small_twiddles_acquire(int field, uint32_t log_n, const uint64_t* root, zntt_twiddles** out);
+int small_twiddles_release(zntt_twiddles* tw);
+int small_ntt_device(const zntt_twiddles* tw, const uint64_t* d_src, uint64_t* d_dst, uint64_t* d_scratch, int mode,
+                     void* stream);
+void small_shutdown();
+
+}  // namespace zntt
