@@ -173,16 +173,21 @@ def cpu_oracle(native: bool = True):
     return O, lib
 
 
-def cpu_transform_seconds(O, lib, data, log_n, stages, workers):
-    """One in-place oracle nttWithTwiddles over `data`, fork-join over `workers` threads."""
+def cpu_transform_seconds(O, lib, data, log_n, stages, workers, field=None):
+    """One in-place oracle nttWithTwiddles over `data` (BN254-Fr 4-u64 slots, or one u64 per
+    element for a 64-bit `field`), fork-join over `workers` threads."""
     ptrs = (O._U64P * len(stages))()
     lens = (ctypes.c_size_t * len(stages))()
     for s, a in enumerate(stages):
         ptrs[s] = a.ctypes.data_as(O._U64P)
         lens[s] = len(a)
     t0 = time.perf_counter()
-    st = lib.zo_ntt_with_twiddles_inplace4(O.BN254_FR, O._p(data), len(data), log_n, ptrs, lens, len(stages), 0,
-                                           workers)
+    if field is None:
+        st = lib.zo_ntt_with_twiddles_inplace4(O.BN254_FR, O._p(data), len(data), log_n, ptrs, lens, len(stages), 0,
+                                               workers)
+    else:
+        st = lib.zo_ntt_with_twiddles_inplace1(field, data.ctypes.data_as(O._U64P), len(data), log_n, ptrs, lens,
+                                               len(stages), 0, workers)
     dt = time.perf_counter() - t0
     assert st == 0
     return dt
@@ -358,6 +363,8 @@ def run_zntt(args, rank, world, local):
             extra["coset_lde"] = run_lde_config(z, torch, stream, steps=5, warmup=2)
             extra["poly_mul"] = run_poly_config(z, torch, stream, steps=5, warmup=2,
                                                 cpu_sample=not args.no_cpu_baseline)
+            extra["small_fields"] = run_small_config(z, torch, stream, steps=20, warmup=3,
+                                                     cpu_sample=not args.no_cpu_baseline)
     if pg:
         pg.barrier()
         pg.destroy_process_group()
@@ -601,6 +608,57 @@ def cpu_schoolbook_sample(n_full, log_sample=12):
             "extrapolated_ms_full": n_full * n_full / rate * 1e3}
 
 
+def run_small_config(z, torch, stream, steps, warmup, log_n=24, cpu_sample=True):
+    """Goldilocks and BabyBear (zig-field's SmallField, 8-byte canonical elements) forward
+    transforms of 2^log_n with the device-resident API.  These are memory- and issue-bound,
+    not multiply-bound: the roofline is HBM bytes moved by the passes against the measured
+    copy bandwidth."""
+    import numpy as np
+    sptr = stream.cuda_stream
+    n = 1 << log_n
+    peaks, hbm_src = measured_peaks()
+    hbm_peak = float(peaks["hbm_gbs"])
+    out = {"workload": f"forward transform of 2^{log_n} canonical u64 elements per field", "fields": {}}
+    for F in (z.GOLDILOCKS, z.BABYBEAR):
+        xs = np.random.default_rng(77).integers(0, F.modulus, n, dtype=np.uint64)
+        x = torch.from_numpy(xs.view(np.int64)).cuda()
+        y = torch.empty_like(x)
+        torch.cuda.synchronize()
+        with z.DeviceTwiddles(F, log_n, z.primitiveRootOfUnity(F, log_n)) as tw:
+            run = lambda: z.ntt_device(tw, x.data_ptr(), y.data_ptr(), z.FORWARD, stream=sptr)  # noqa: E731
+            for _ in range(warmup):
+                run()
+            ms = time_region(torch, stream, run, steps) / steps
+        passes = 1 if log_n <= 12 else -(-log_n // 10)
+        moved = passes * 2 * 8 * n
+        r = {"ms": ms, "value": n / (ms * 1e-3), "unit": "elements/s", "passes": passes,
+             "hbm": {"achieved": moved / (ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": moved / (ms * 1e-3) / 1e9 / hbm_peak, "bytes_per_transform": moved,
+                     "peak_source": hbm_src}}
+        if cpu_sample:
+            r["cpu_baseline"] = cpu_small_sample(F, xs, log_n)
+        out["fields"][F.name] = r
+        del x, y
+    return out
+
+
+def cpu_small_sample(F, xs, log_n):
+    """The oracle's nttWithTwiddles on all host cores for one full transform (Montgomery form
+    inside the oracle; conversion excluded from the time)."""
+    import numpy as np
+    O, lib = cpu_oracle(native=True)
+    fid = {"goldilocks": O.GOLDILOCKS, "babybear": O.BABYBEAR}[F.name]
+    workers = min(os.cpu_count() or 1, 64)
+    slots = O.elems(len(xs))
+    slots[:, 0] = xs
+    data = np.ascontiguousarray(O.to_mont(fid, slots)[:, 0])  # one u64 per element, Montgomery form
+    st, root = O.primitive_root(fid, log_n)
+    st, stages = O.precompute_twiddles(fid, log_n, root)
+    dt = cpu_transform_seconds(O, lib, data, log_n, stages, workers, field=fid)
+    return {"value": len(xs) / dt, "unit": "elements/s", "cores": workers, "kind": "port",
+            "sample": f"one full 2^{log_n} forward transform, oracle nttWithTwiddles, fork-join over butterflies"}
+
+
 def cpu_baseline_sample(host_data, log_n):
     """The oracle port on all host cores, on the same input, for one full transform."""
     workers = min(os.cpu_count() or 1, 64)
@@ -678,6 +736,12 @@ def run_single_config(args):
         if args.workload == "batched":
             r = run_batched_config(z, torch, stream, steps=args.steps, warmup=args.warmup)
             metric = "batched BN254-Fr NTT elems/s (512 x 2^U{10..16} + 8 x 2^20)"
+        elif args.workload == "small":
+            r = run_small_config(z, torch, stream, steps=args.steps, warmup=args.warmup,
+                                 cpu_sample=not args.no_cpu_baseline)
+            r["value"] = r["fields"]["goldilocks"]["value"]
+            r["unit"] = "elements/s"
+            metric = "Goldilocks NTT elems/s at 2^24 (BabyBear beside it)"
         elif args.workload == "poly":
             r = run_poly_config(z, torch, stream, steps=args.steps, warmup=args.warmup,
                                 cpu_sample=not args.no_cpu_baseline)
@@ -701,8 +765,8 @@ def main():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true",
-                    help="skip the batched, coset-extension and polynomial-product lines")
-    ap.add_argument("--workload", default="ntt", choices=["ntt", "serve", "batched", "lde", "poly"])
+                    help="skip the batched, coset-extension, polynomial-product and small-field lines")
+    ap.add_argument("--workload", default="ntt", choices=["ntt", "serve", "batched", "lde", "poly", "small"])
     ap.add_argument("--serve-requests", type=int, default=20000)
     ap.add_argument("--serve-sweep", type=float, nargs="*", default=[8000.0, 32000.0])
     ap.add_argument("--serve-sweep-requests", type=int, default=6000)
@@ -712,7 +776,7 @@ def main():
         if rank == 0:
             run_serve(args)
         return
-    if args.workload in ("batched", "lde", "poly"):
+    if args.workload in ("batched", "lde", "poly", "small"):
         if rank == 0:
             run_single_config(args)
         return

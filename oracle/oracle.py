@@ -79,6 +79,7 @@ def load(path: str | None = None):
     lib.zo_ntt_with_twiddles.argtypes = [i, _U64P, sz, sz, ctypes.POINTER(_U64P),
                                          ctypes.POINTER(sz), sz, i, i]
     lib.zo_ntt_with_twiddles_inplace4.argtypes = lib.zo_ntt_with_twiddles.argtypes
+    lib.zo_ntt_with_twiddles_inplace1.argtypes = lib.zo_ntt_with_twiddles.argtypes
     lib.zo_chacha20_stream.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_void_p, sz]
     lib.zo_random_elements.argtypes = [i, ctypes.c_char_p, _U64P, sz]
     lib.zo_powers.argtypes = [i, _U64P, _U64P, sz]

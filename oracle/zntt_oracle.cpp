@@ -936,6 +936,17 @@ int zo_ntt_with_twiddles_inplace4(int field, uint64_t* data, size_t len, size_t 
                               inverse != 0, workers);
 }
 
+// The same for the 64-bit fields (Goldilocks, BabyBear): `data` holds one
+// u64 per element (Montgomery form); stages are 4-u64 slots as elsewhere.
+int zo_ntt_with_twiddles_inplace1(int field, uint64_t* data, size_t len, size_t log_n,
+                                  const uint64_t* const* stages, const size_t* lens,
+                                  size_t num_stages, int inverse, int workers) {
+  if (field != ZO_GOLDILOCKS && field != ZO_BABYBEAR) return ZO_UNSUPPORTED_FIELD;
+  const Mont<1>& F = field == ZO_GOLDILOCKS ? goldilocks() : babybear();
+  return ntt_with_twiddles<1>(F, reinterpret_cast<Elem<1>*>(data), len, log_n, stages, lens, num_stages,
+                              inverse != 0, workers);
+}
+
 int zo_chacha20_stream(const uint8_t* seed32, const uint8_t* nonce12, uint8_t* out, size_t len) {
   ChaCha c;
   uint8_t zero_nonce[12] = {0};

@@ -4,8 +4,10 @@
 //! The seven public functions keep zig-ntt's names, parameters and error
 //! names; the error sets gain `DeviceError` and `OutOfMemory` (a GPU can fail
 //! where a CPU loop cannot).  `F` must be BN254-Fr or BLS12-381-Fr with
-//! zig-field's `BigField` layout (four u64 Montgomery limbs at offset 0); any
-//! other field is a compile error, since there is deliberately no CPU path.
+//! zig-field's `BigField` layout (four u64 Montgomery limbs at offset 0), or
+//! Goldilocks or BabyBear with its `SmallField` layout (one canonical u64,
+//! `value`); any other field is a compile error, since there is deliberately
+//! no CPU path.
 //!
 //! Written for Zig 0.16.0 (the reference's toolchain); it was not compiled
 //! in the environment this library was built in, which has no Zig.
@@ -19,6 +21,7 @@ const ZStage = extern struct {
 
 extern fn zntt_init(device: c_int) c_int;
 extern fn zntt_bit_reverse(data: [*]u64, len: usize) c_int;
+extern fn zntt_bit_reverse_small(data: [*]u64, len: usize) c_int;
 extern fn zntt_ntt(field: c_int, data: [*]u64, len: usize, log_n: usize, root: *const [4]u64) c_int;
 extern fn zntt_intt(field: c_int, data: [*]u64, len: usize, log_n: usize, root: *const [4]u64) c_int;
 extern fn zntt_precompute_twiddles(field: c_int, log_n: usize, root: *const [4]u64, stage_out: [*]const [*]u64) c_int;
@@ -29,15 +32,28 @@ extern fn zntt_poly_mul(field: c_int, a: [*]const u64, a_len: usize, b: [*]const
 
 const BN254_FR: u512 = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001;
 const BLS12_381_FR: u512 = 0x73EDA753299D7D483339D80809A1D80553BDA402FFFE5BFEFFFFFFFF00000001;
+const GOLDILOCKS: u64 = 0xFFFFFFFF00000001;
+const BABYBEAR: u64 = 0x78000001;
+
+/// `F` is a SmallField (one canonical u64 per element) rather than a BigField.
+fn isSmall(comptime F: type) bool {
+    return comptime @hasField(F, "value") and @sizeOf(F) == 8;
+}
 
 /// The library's field id for `F`, checked at compile time.
 fn fieldId(comptime F: type) c_int {
     comptime {
+        if (isSmall(F)) {
+            if (@offsetOf(F, "value") != 0) @compileError("zig-ntt on B200 needs SmallField's u64 layout");
+            if (F.MODULUS == GOLDILOCKS) return 2;
+            if (F.MODULUS == BABYBEAR) return 3;
+            @compileError("zig-ntt on B200 supports Goldilocks and BabyBear among the small fields");
+        }
         if (@sizeOf(F) != 32 or @offsetOf(F, "limbs") != 0 or F.NUM_LIMBS != 4)
             @compileError("zig-ntt on B200 needs a 4x u64 Montgomery field");
         if (F.MODULUS == BN254_FR) return 0;
         if (F.MODULUS == BLS12_381_FR) return 1;
-        @compileError("zig-ntt on B200 supports BN254-Fr and BLS12-381-Fr only");
+        @compileError("zig-ntt on B200 supports BN254-Fr, BLS12-381-Fr, Goldilocks and BabyBear");
     }
 }
 
@@ -59,8 +75,10 @@ fn limbs(comptime F: type, data: []F) [*]u64 {
     return @ptrCast(data.ptr);
 }
 
-fn rootLimbs(comptime F: type, root: *const F) *const [4]u64 {
-    return @ptrCast(&root.limbs);
+/// A root as the C ABI takes it: four limbs, or a small field's value then zeros.
+fn rootLimbs(comptime F: type, root: *const F) [4]u64 {
+    if (comptime isSmall(F)) return .{ root.value, 0, 0, 0 };
+    return root.limbs;
 }
 
 /// zig-ntt's `sizeFromLog` (root.zig:33-36).
@@ -86,7 +104,8 @@ pub fn bitReverse(comptime F: type, data: []F) error{ InvalidLength, DeviceError
     const n = data.len;
     if (n == 0 or (n & (n - 1)) != 0) return error.InvalidLength;
     try ensureInit();
-    return @errorCast(mapStatus(zntt_bit_reverse(limbs(F, data), n)));
+    const status = if (comptime isSmall(F)) zntt_bit_reverse_small(limbs(F, data), n) else zntt_bit_reverse(limbs(F, data), n);
+    return @errorCast(mapStatus(status));
 }
 
 pub fn ntt(comptime F: type, data: []F, log_n: usize, root: F) error{ LogTooLarge, LengthMismatch, InvalidLength, DeviceError, OutOfMemory }!void {
@@ -94,7 +113,7 @@ pub fn ntt(comptime F: type, data: []F, log_n: usize, root: F) error{ LogTooLarg
     const n = try sizeFromLog(log_n);
     if (data.len != n) return error.LengthMismatch;
     try ensureInit();
-    return @errorCast(mapStatus(zntt_ntt(id, limbs(F, data), data.len, log_n, rootLimbs(F, &root))));
+    return @errorCast(mapStatus(zntt_ntt(id, limbs(F, data), data.len, log_n, &rootLimbs(F, &root))));
 }
 
 pub fn intt(comptime F: type, data: []F, log_n: usize, root: F) error{ LogTooLarge, LengthMismatch, InvalidLength, DeviceError, OutOfMemory }!void {
@@ -102,7 +121,7 @@ pub fn intt(comptime F: type, data: []F, log_n: usize, root: F) error{ LogTooLar
     const n = try sizeFromLog(log_n);
     if (data.len != n) return error.LengthMismatch;
     try ensureInit();
-    return @errorCast(mapStatus(zntt_intt(id, limbs(F, data), data.len, log_n, rootLimbs(F, &root))));
+    return @errorCast(mapStatus(zntt_intt(id, limbs(F, data), data.len, log_n, &rootLimbs(F, &root))));
 }
 
 /// Allocates the table exactly as zig-ntt does (`log_n` stages, stage s of
@@ -123,7 +142,7 @@ pub fn precomputeTwiddles(comptime F: type, log_n: usize, root: F, allocator: st
         ptrs[s] = @ptrCast(twiddles[s].ptr);
     }
     try ensureInit();
-    try @as(error{ LogTooLarge, OutOfMemory, DeviceError }!void, @errorCast(mapStatus(zntt_precompute_twiddles(id, log_n, rootLimbs(F, &root), &ptrs))));
+    try @as(error{ LogTooLarge, OutOfMemory, DeviceError }!void, @errorCast(mapStatus(zntt_precompute_twiddles(id, log_n, &rootLimbs(F, &root), &ptrs))));
     return twiddles;
 }
 
