@@ -73,8 +73,9 @@ __device__ __forceinline__ uint32_t rev_bits_small(uint32_t x, uint32_t bits) {
 
 // Twiddle of global stage s for butterfly jg: forward tw[s-1][jg], inverse 1
 // (jg = 0) or -tw[s-1][2^(s-1) - jg] (root.zig:199); false when it is one.
+// Indices are 32-bit: transforms are at most 2^31 elements.
 template <class SF>
-__device__ __forceinline__ bool small_twiddle(const SmallPass& pp, const uint64_t* stw, uint64_t half, uint64_t jg,
+__device__ __forceinline__ bool small_twiddle(const SmallPass& pp, const uint64_t* stw, uint32_t half, uint32_t jg,
                                               uint64_t& w) {
   if (jg == 0 && (pp.inverse | pp.tw0_one)) return false;
   w = pp.inverse ? SF::neg(__ldg(stw + (half - jg))) : __ldg(stw + jg);
@@ -95,14 +96,14 @@ __global__ void __launch_bounds__(THREADS) small_pass_kernel(SmallPass pp) {
   const uint32_t k = pp.k, c = pp.c, C = 1u << c;
   const uint32_t tile = 1u << (k + c);
   const uint32_t tid = threadIdx.x;
-  const uint64_t blk = blockIdx.x;
-  uint64_t hi_base = 0, m0 = 0, col0 = 0;
+  const uint32_t blk = blockIdx.x;
+  uint32_t hi_base = 0, m0 = 0, col0 = 0;
   if (pp.first) {
     col0 = blk << c;
   } else {
     const uint32_t mlog = pp.S - c;
     hi_base = (blk >> mlog) << (pp.S + k);
-    m0 = (blk & ((1ull << mlog) - 1)) << c;
+    m0 = (blk & ((1u << mlog) - 1)) << c;
   }
   const uint32_t xcols_log = pp.log_n - k;
 
@@ -111,13 +112,12 @@ __global__ void __launch_bounds__(THREADS) small_pass_kernel(SmallPass pp) {
     const uint32_t e = tid + q * THREADS;
     if (e < tile) {
       const uint32_t col = e & (C - 1), row = e >> c;
-      uint64_t g;
-      uint32_t t;
+      uint32_t g, t;
       if (pp.first) {
-        g = ((uint64_t)row << xcols_log) + col0 + col;
+        g = (row << xcols_log) + col0 + col;
         t = rev_bits_small(row, k);
       } else {
-        g = hi_base + ((uint64_t)row << pp.S) + m0 + col;
+        g = hi_base + (row << pp.S) + m0 + col;
         t = row;
       }
       sm[(t << c) | col] = pp.src[g];
@@ -127,14 +127,14 @@ __global__ void __launch_bounds__(THREADS) small_pass_kernel(SmallPass pp) {
 
   uint32_t i = 1;
   if (k & 1) {
-    const uint64_t half = 1ull << pp.S;
+    const uint32_t half = 1u << pp.S;
     const uint64_t* stw = pp.tw + (half - 1);
 #pragma unroll
     for (uint32_t q = 0; q < TILE_MAX / 2 / THREADS; q++) {
       const uint32_t b = tid + q * THREADS;
       if (b < tile / 2) {
         const uint32_t col = b & (C - 1), t0 = (b >> c) << 1;
-        const uint64_t jg = pp.first ? 0 : m0 + col;
+        const uint32_t jg = pp.first ? 0 : m0 + col;
         const uint32_t e0 = (t0 << c) | col, e1 = e0 + C;
         uint64_t u = sm[e0], v = sm[e1], w = 0;
         const bool mul = small_twiddle<SF>(pp, stw, half, jg, w);
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(THREADS) small_pass_kernel(SmallPass pp) {
   }
   for (; i < k; i += 2) {
     const uint32_t h = 1u << (i - 1);
-    const uint64_t half1 = 1ull << (pp.S + i - 1), half2 = half1 << 1;
+    const uint32_t half1 = 1u << (pp.S + i - 1), half2 = half1 << 1;
     const uint64_t* stw1 = pp.tw + (half1 - 1);
     const uint64_t* stw2 = pp.tw + (half2 - 1);
 #pragma unroll
@@ -159,13 +159,13 @@ __global__ void __launch_bounds__(THREADS) small_pass_kernel(SmallPass pp) {
         const uint32_t j = g & (h - 1);
         const uint32_t t0 = ((g >> (i - 1)) << (i + 1)) | j;
         const uint32_t e0 = (t0 << c) | col, eh = h << c;
-        uint64_t jg1, jg3;
+        uint32_t jg1, jg3;
         if (pp.first) {
           jg1 = j;
           jg3 = j + h;
         } else {
-          jg1 = ((uint64_t)j << pp.S) + m0 + col;
-          jg3 = jg1 + ((uint64_t)h << pp.S);
+          jg1 = (j << pp.S) + m0 + col;
+          jg3 = jg1 + (h << pp.S);
         }
         uint64_t w1 = 0, w2 = 0, w3 = 0;
         const bool m1 = small_twiddle<SF>(pp, stw1, half1, jg1, w1);
@@ -190,8 +190,8 @@ __global__ void __launch_bounds__(THREADS) small_pass_kernel(SmallPass pp) {
     const uint32_t e = tid + q * THREADS;
     if (e < tile) {
       const uint32_t col = e & (C - 1), row = e >> c;
-      const uint64_t g = pp.first ? ((uint64_t)rev_bits_small((uint32_t)(col0 + col), xcols_log) << k) + row
-                                  : hi_base + ((uint64_t)row << pp.S) + m0 + col;
+      const uint32_t g = pp.first ? (rev_bits_small(col0 + col, xcols_log) << k) + row
+                                  : hi_base + (row << pp.S) + m0 + col;
       uint64_t x = sm[(row << c) | col];
       if (pp.scale) x = SF::mul(pp.scale_val, x);
       pp.dst[g] = x;

@@ -21,31 +21,88 @@ struct Goldilocks {
   static constexpr uint64_t P = 0xFFFFFFFF00000001ull;
   static constexpr uint64_t EPS = 0xFFFFFFFFull;  // 2^64 mod p = 2^32 - 1
 
-  __device__ __forceinline__ static uint64_t add(uint64_t a, uint64_t b) {
-    uint64_t s = a + b;
-    // a + b < 2p: a carry out of 64 bits means s + 2^64 = s + EPS (mod p),
-    // which is then below p; otherwise subtract p once if needed.
-    if (s < a) return s + EPS;
-    return s >= P ? s - P : s;
+  // The arithmetic runs on 32-bit halves with carry chains: a 64-bit compare
+  // and select costs several ALU instructions, a carry flag none.
+  __device__ __forceinline__ static uint64_t join(uint32_t lo, uint32_t hi) {
+    return ((uint64_t)hi << 32) | lo;
   }
+  // x - p when x >= p, else x, for x = (hi:lo) below 2^64.
+  __device__ __forceinline__ static uint64_t reduce_once(uint32_t lo, uint32_t hi) {
+    uint32_t d0, d1, br;
+    asm("sub.cc.u32  %0, %3, 1;\n\t"
+        "subc.cc.u32 %1, %4, 0xFFFFFFFF;\n\t"
+        "subc.u32    %2, 0, 0;"
+        : "=r"(d0), "=r"(d1), "=r"(br)
+        : "r"(lo), "r"(hi));
+    return br ? join(lo, hi) : join(d0, d1);
+  }
+  // a + b < 2p: the 65-bit sum less p, unless that borrows.
+  __device__ __forceinline__ static uint64_t add(uint64_t a, uint64_t b) {
+    uint32_t s0, s1, c, d0, d1, br;
+    asm("add.cc.u32  %0, %3, %5;\n\t"
+        "addc.cc.u32 %1, %4, %6;\n\t"
+        "addc.u32    %2, 0, 0;"
+        : "=r"(s0), "=r"(s1), "=r"(c)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    asm("sub.cc.u32  %0, %3, 1;\n\t"
+        "subc.cc.u32 %1, %4, 0xFFFFFFFF;\n\t"
+        "subc.u32    %2, %5, 0;"
+        : "=r"(d0), "=r"(d1), "=r"(br)
+        : "r"(s0), "r"(s1), "r"(c));
+    return br ? join(s0, s1) : join(d0, d1);
+  }
+  // a - b, plus p (low word 1, high word 2^32 - 1) when it borrows.
   __device__ __forceinline__ static uint64_t sub(uint64_t a, uint64_t b) {
-    const uint64_t d = a - b;
-    // a < b: the wrapped difference is a - b + 2^64; adding p is subtracting EPS.
-    return a < b ? d - EPS : d;
+    uint32_t d0, d1, br;
+    asm("sub.cc.u32  %0, %3, %5;\n\t"
+        "subc.cc.u32 %1, %4, %6;\n\t"
+        "subc.u32    %2, 0, 0;"
+        : "=r"(d0), "=r"(d1), "=r"(br)
+        : "r"((uint32_t)a), "r"((uint32_t)(a >> 32)), "r"((uint32_t)b), "r"((uint32_t)(b >> 32)));
+    asm("add.cc.u32  %0, %0, %2;\n\t"
+        "addc.u32    %1, %1, %3;"
+        : "+r"(d0), "+r"(d1)
+        : "r"(br & 1u), "r"(br));
+    return join(d0, d1);
   }
   __device__ __forceinline__ static uint64_t neg(uint64_t a) { return a == 0 ? 0 : P - a; }
-  // a * b mod p from the 128-bit product hi * 2^64 + lo with hi = h1 * 2^32 + h0:
-  // 2^64 = 2^32 - 1 and 2^96 = -1 (mod p), so the product is
-  // lo - h1 + h0 * (2^32 - 1) (mod p).
+  // a * b mod p.  The 128-bit product is z3:z2:z1:z0 (32-bit words); with
+  // 2^64 = 2^32 - 1 and 2^96 = -1 (mod p) it is (z1:z0) + z2 * 2^32 - z2 - z3.
+  // That sum is c * 2^64 + t with c in {-1, 0, 1}; c * 2^64 = c * (2^32 - 1),
+  // added to t as a 64-bit two's-complement term (lo -c, hi c >> 31), cannot
+  // leave [0, 2^64): for c = 1, t <= 2^64 - 2^32 - 1; for c = -1, t >= 2^64 - 2^33.
   __device__ __forceinline__ static uint64_t mul(uint64_t a, uint64_t b) {
-    const uint64_t lo = a * b, hi = __umul64hi(a, b);
-    const uint64_t h0 = hi & 0xFFFFFFFFull, h1 = hi >> 32;
-    uint64_t t = lo - h1;
-    if (lo < h1) t -= EPS;  // borrow: add p
-    const uint64_t u = (h0 << 32) - h0;
-    uint64_t r = t + u;
-    if (r < t) r += EPS;  // carry: 2^64 = EPS (mod p); cannot carry again
-    return r >= P ? r - P : r;
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    uint32_t z0, z1, z2, z3;
+    asm("mul.lo.u32     %0, %4, %6;\n\t"
+        "mul.hi.u32     %1, %4, %6;\n\t"
+        "mul.lo.u32     %2, %5, %7;\n\t"
+        "mul.hi.u32     %3, %5, %7;\n\t"
+        "mad.lo.cc.u32  %1, %4, %7, %1;\n\t"
+        "madc.hi.cc.u32 %2, %4, %7, %2;\n\t"
+        "addc.u32       %3, %3, 0;\n\t"
+        "mad.lo.cc.u32  %1, %5, %6, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+        "addc.u32       %3, %3, 0;"
+        : "=r"(z0), "=r"(z1), "=r"(z2), "=r"(z3)
+        : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+    uint32_t t0, t1, c, w0, w1;
+    asm("add.cc.u32  %0, %2, %3;\n\t"   // w = z2 + z3 (33 bits)
+        "addc.u32    %1, 0, 0;"
+        : "=r"(w0), "=r"(w1)
+        : "r"(z2), "r"(z3));
+    asm("add.cc.u32  %1, %4, %5;\n\t"   // (c:t1:t0) = (z1:z0) + z2 * 2^32 ...
+        "addc.u32    %2, 0, 0;\n\t"
+        "sub.cc.u32  %0, %3, %6;\n\t"   // ... - w
+        "subc.cc.u32 %1, %1, %7;\n\t"
+        "subc.u32    %2, %2, 0;"
+        : "=r"(t0), "=r"(t1), "=r"(c)
+        : "r"(z0), "r"(z1), "r"(z2), "r"(w0), "r"(w1));
+    asm("add.cc.u32  %0, %0, %2;\n\t"
+        "addc.u32    %1, %1, %3;"
+        : "+r"(t0), "+r"(t1)
+        : "r"(0u - c), "r"((uint32_t)((int32_t)c >> 31)));
+    return reduce_once(t0, t1);
   }
 };
 
