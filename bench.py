@@ -365,6 +365,7 @@ def run_zntt(args, rank, world, local):
                                                 cpu_sample=not args.no_cpu_baseline)
             extra["small_fields"] = run_small_config(z, torch, stream, steps=20, warmup=3,
                                                      cpu_sample=not args.no_cpu_baseline)
+            extra["fri_fold"] = run_fri_config(z, torch, stream, steps=20, warmup=3)
     if pg:
         pg.barrier()
         pg.destroy_process_group()
@@ -642,6 +643,53 @@ def run_small_config(z, torch, stream, steps, warmup, log_n=24, cpu_sample=True)
     return out
 
 
+def run_fri_config(z, torch, stream, steps, warmup, log_n=24):
+    """FRI fold rounds (libs/fri/src/root.zig:396-403) on resident evaluations: one fold of a
+    2^log_n layer, and the whole chain 2^log_n -> 2^10 sharing one table, for BN254-Fr and
+    Goldilocks.  A fold reads the layer and the 1/(2x) table and writes half a layer."""
+    import numpy as np
+    sptr = stream.cuda_stream
+    peaks, hbm_src = measured_peaks()
+    hbm_peak = float(peaks["hbm_gbs"])
+    out = {"workload": f"FRI fold of a 2^{log_n}-evaluation layer, and the chain 2^{log_n} -> 2^10",
+           "fields": {}}
+    for F in (z.BN254_FR, z.GOLDILOCKS):
+        ew = 8 * F.limbs  # bytes per element
+        n = 1 << log_n
+        layer = torch.empty(n * F.limbs, dtype=torch.int64, device="cuda")
+        if F.limbs == 4:
+            z.random_elements(F, 91, layer.data_ptr(), n, stream=sptr)
+        else:
+            xs = np.random.default_rng(91).integers(0, F.modulus, n, dtype=np.uint64)
+            layer.copy_(torch.from_numpy(xs.view(np.int64)))
+        bufs = [torch.empty((n >> (r + 1)) * F.limbs, dtype=torch.int64, device="cuda") for r in range(log_n - 10)]
+        alpha = z.to_montgomery(F, 987654321) if F.limbs == 4 else np.array([987654321, 0, 0, 0], dtype=np.uint64)
+        torch.cuda.synchronize()
+        one = lambda: z.fri_fold(F, layer.data_ptr(), log_n, alpha, bufs[0].data_ptr(), log_table=log_n,  # noqa: E731
+                                 stream=sptr)
+
+        def chain():
+            src = layer
+            for r, dst in enumerate(bufs):
+                z.fri_fold(F, src.data_ptr(), log_n - r, alpha, dst.data_ptr(), log_table=log_n, stream=sptr)
+                src = dst
+
+        for _ in range(warmup):
+            one()
+            chain()
+        ms_one = time_region(torch, stream, one, steps) / steps
+        ms_chain = time_region(torch, stream, chain, steps) / steps
+        moved = (n + n // 2 + n // 2) * ew  # layer read, table read, half layer written
+        out["fields"][F.name] = {
+            "fold_ms": ms_one, "fold_value": (n // 2) / (ms_one * 1e-3), "unit": "output elements/s",
+            "hbm": {"achieved": moved / (ms_one * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": moved / (ms_one * 1e-3) / 1e9 / hbm_peak, "peak_source": hbm_src},
+            "chain_rounds": log_n - 10, "chain_ms": ms_chain,
+        }
+        del layer, bufs
+    return out
+
+
 def cpu_small_sample(F, xs, log_n):
     """The oracle's nttWithTwiddles on all host cores for one full transform (Montgomery form
     inside the oracle; conversion excluded from the time)."""
@@ -742,6 +790,11 @@ def run_single_config(args):
             r["value"] = r["fields"]["goldilocks"]["value"]
             r["unit"] = "elements/s"
             metric = "Goldilocks NTT elems/s at 2^24 (BabyBear beside it)"
+        elif args.workload == "fri":
+            r = run_fri_config(z, torch, stream, steps=args.steps, warmup=args.warmup)
+            r["value"] = r["fields"]["bn254_fr"]["fold_value"]
+            r["unit"] = "output elements/s"
+            metric = "BN254-Fr FRI fold output elems/s (2^24 -> 2^23; Goldilocks beside it)"
         elif args.workload == "poly":
             r = run_poly_config(z, torch, stream, steps=args.steps, warmup=args.warmup,
                                 cpu_sample=not args.no_cpu_baseline)
@@ -765,8 +818,8 @@ def main():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true",
-                    help="skip the batched, coset-extension, polynomial-product and small-field lines")
-    ap.add_argument("--workload", default="ntt", choices=["ntt", "serve", "batched", "lde", "poly", "small"])
+                    help="skip the batched, coset-extension, polynomial-product, small-field and FRI lines")
+    ap.add_argument("--workload", default="ntt", choices=["ntt", "serve", "batched", "lde", "poly", "small", "fri"])
     ap.add_argument("--serve-requests", type=int, default=20000)
     ap.add_argument("--serve-sweep", type=float, nargs="*", default=[8000.0, 32000.0])
     ap.add_argument("--serve-sweep-requests", type=int, default=6000)
@@ -776,7 +829,7 @@ def main():
         if rank == 0:
             run_serve(args)
         return
-    if args.workload in ("batched", "lde", "poly", "small"):
+    if args.workload in ("batched", "lde", "poly", "small", "fri"):
         if rank == 0:
             run_single_config(args)
         return

@@ -223,6 +223,27 @@ int zntt_poly_mul_device(const zntt_twiddles* tw, const uint64_t* d_a, size_t le
 int zntt_poly_mul(int field, const uint64_t* a, size_t a_len, const uint64_t* b, size_t b_len, size_t max_degree,
                   uint64_t* out, int64_t* out_degree);
 
+/* ---- FRI on resident evaluations ------------------------------------------------
+ * The data-parallel steps of zig-fri's prover (libs/fri/src/root.zig), so a coset
+ * extension's output can be folded without leaving the device.  All four fields;
+ * elements in the field's layout (four Montgomery limbs, or one canonical u64 for
+ * Goldilocks / BabyBear); scalars as uint64_t[4]. */
+
+/* Domain(F).fill (libs/fri/src/root.zig:155-166): d_out[i] = g^i for i < 2^log_n, g the
+ * generator of the order-2^log_n subgroup (the field's primitiveRootOfUnity(log_n)).
+ * ZNTT_ERR_ORDER_TOO_LARGE beyond the two-adicity (Domain.init's DomainTooLarge). */
+int zntt_fri_domain_fill(int field, uint32_t log_n, uint64_t* d_out, void* stream);
+
+/* One fold round of proveOn (libs/fri/src/root.zig:396-403) on a layer of 2^log_n
+ * evaluations in natural order on the order-2^log_n subgroup:
+ *   d_out[j] = (f[j] + f[j + n/2]) / 2 + alpha * (f[j] - f[j + n/2]) / (2 g^j),  j < n/2.
+ * The factors 1/(2 g^j) come from a device table kept per (field, log_table), log_table
+ * being the size of the largest layer folded with it (0: log_n); pass the first layer's
+ * size for every round of one proof so that all rounds share one table.  Stream-ordered;
+ * d_out must not overlap the layer. */
+int zntt_fri_fold_device(int field, const uint64_t* d_layer, uint32_t log_n, const uint64_t alpha[4],
+                         uint64_t* d_out, uint32_t log_table, void* stream);
+
 /* ---- serving: a continuously batching request server ---------------------------
  * Requests carry pinned host buffers.  A worker thread admits them in FIFO
  * order while their device buffers fit the HBM budget, turns whatever is

@@ -87,6 +87,8 @@ def load(path: str | None = None):
     lib.zo_dft_points.argtypes = [i, _U64P, sz, _U64P, _U64P, sz, _U64P, i]
     lib.zo_poly_mul.argtypes = [i, _U64P, sz, _U64P, sz, sz, _U64P, ctypes.POINTER(ctypes.c_int64), i]
     lib.zo_poly_eval.argtypes = [i, _U64P, sz, _U64P, sz, _U64P, i]
+    lib.zo_fri_domain_fill.argtypes = [i, sz, _U64P]
+    lib.zo_fri_fold.argtypes = [i, _U64P, sz, _U64P, _U64P, i]
     if path.endswith("liboracle.so"):
         _lib = lib
     return lib
@@ -273,5 +275,22 @@ def poly_eval(field: int, c: np.ndarray, xs: np.ndarray, workers: int = 1) -> np
     out = elems(len(xs))
     st = load().zo_poly_eval(field, _p(np.ascontiguousarray(c)), len(c), _p(np.ascontiguousarray(xs)), len(xs),
                              _p(out), workers)
+    assert st == OK, st
+    return out
+
+
+def fri_domain_fill(field: int, log_n: int) -> np.ndarray:
+    """Domain(F).fill (libs/fri/src/root.zig:155-166): g^i for i < 2^log_n (Montgomery slots)."""
+    out = elems(1 << log_n)
+    st = load().zo_fri_domain_fill(field, log_n, _p(out))
+    assert st == OK, st
+    return out
+
+
+def fri_fold(field: int, layer: np.ndarray, log_n: int, alpha: np.ndarray, workers: int = 1) -> np.ndarray:
+    """One fold round of proveOn (libs/fri/src/root.zig:396-403) on 2^log_n slots."""
+    out = elems(1 << (log_n - 1))
+    a = np.ascontiguousarray(np.asarray(alpha, dtype=np.uint64).reshape(1, 4))
+    st = load().zo_fri_fold(field, _p(np.ascontiguousarray(layer)), log_n, _p(a), _p(out), workers)
     assert st == OK, st
     return out

@@ -22,6 +22,7 @@
 //   libs/rng/src/rng.zig:32-65             randomFieldElement (big-endian rejection draw)
 //   libs/poly/src/vector.zig:24-32,68-73   powers / hadamard (coset LDE composition)
 //   libs/poly/src/poly.zig:76-107,197-224  fromCoeffs / normalize / mul (schoolbook) / eval
+//   libs/fri/src/root.zig:133-166,396-403  Domain.init / at / fill and the proveOn fold round
 //   libs/parallel/src/root.zig:45-79       parallelFor fork-join semantics (harness only)
 //
 // The reference is Zig 0.16 and cannot be compiled in this environment; the
@@ -1134,6 +1135,76 @@ int zo_poly_eval(int field, const uint64_t* c, size_t len, const uint64_t* xs, s
           F.add(t, ci, acc);
         }
         store<N>(out + 4 * q, acc);
+      }
+    });
+    return ZO_OK;
+  });
+}
+
+}  // extern "C"
+
+// Domain(F).init(log_n) (libs/fri/src/root.zig:133-138): omega =
+// primitiveRootOfUnity(two_adicity), step_gen = omega^(2^(two_adicity - log_n)).
+template <class FT, int N>
+static int fri_step_gen(const FT& F, size_t log_n, uint64_t* step) {
+  if ((long)log_n > F.two_adicity) return ZO_ORDER_TOO_LARGE;
+  uint64_t omega[N];
+  int st = F.primitive_root(F.two_adicity, omega);
+  if (st) return st;
+  std::memcpy(step, omega, sizeof(uint64_t) * N);
+  for (size_t i = 0; i < (size_t)F.two_adicity - log_n; i++) F.mul(step, step, step);
+  return ZO_OK;
+}
+
+extern "C" {
+
+// Domain.fill (:155-166): x = one; each slot gets x, then x *= step_gen.
+int zo_fri_domain_fill(int field, size_t log_n, uint64_t* out) {
+  return dispatch(field, [&](const auto& F) -> int {
+    constexpr int N = sizeof(F.P) / sizeof(uint64_t);
+    uint64_t g[N], x[N];
+    int st = fri_step_gen<std::decay_t<decltype(F)>, N>(F, log_n, g);
+    if (st) return st;
+    std::memcpy(x, F.ONE, sizeof(x));
+    for (size_t i = 0; i < ((size_t)1 << log_n); i++) {
+      store<N>(out + 4 * i, x);
+      F.mul(x, g, x);
+    }
+    return ZO_OK;
+  });
+}
+
+// One fold round of proveOn (:396-403): for j < n/2, x = dom.at(j) = step_gen^j,
+// even = (f_j + f_{j+n/2}) * half_inv, odd = (f_j - f_{j+n/2}).div(x) * half_inv,
+// next_j = even + alpha * odd, with half_inv = 1.div(2) and div = mul by inverse.
+int zo_fri_fold(int field, const uint64_t* layer, size_t log_n, const uint64_t* alpha, uint64_t* out, int workers) {
+  return dispatch(field, [&](const auto& F) -> int {
+    constexpr int N = sizeof(F.P) / sizeof(uint64_t);
+    if (log_n < 1) return ZO_LOG_TOO_LARGE;
+    uint64_t g[N], two[N], half_inv[N], a[N];
+    int st = fri_step_gen<std::decay_t<decltype(F)>, N>(F, log_n, g);
+    if (st) return st;
+    F.from_u64(2, two);
+    F.inv(two, half_inv);
+    load<N>(alpha, a);
+    const size_t half = (size_t)1 << (log_n - 1);
+    parallel_for(half, workers, [&](size_t lo, size_t hi) {
+      uint64_t x[N];
+      F.pow_u64(g, lo, x);
+      for (size_t j = lo; j < hi; j++) {
+        uint64_t fx[N], fn[N], s[N], d[N], xi[N], even[N], odd[N], t[N];
+        load<N>(layer + 4 * j, fx);
+        load<N>(layer + 4 * (j + half), fn);
+        F.add(fx, fn, s);
+        F.mul(s, half_inv, even);
+        F.sub(fx, fn, d);
+        F.inv(x, xi);
+        F.mul(d, xi, t);
+        F.mul(t, half_inv, odd);
+        F.mul(a, odd, t);
+        F.add(even, t, t);
+        store<N>(out + 4 * j, t);
+        F.mul(x, g, x);
       }
     });
     return ZO_OK;

@@ -210,6 +210,8 @@ def lib():
         L.zntt_batch_destroy.argtypes = [vp]
         L.zntt_coset_lde_device.argtypes = [vp, vp, _U64P, vp, vp, vp]
         L.zntt_poly_mul_device.argtypes = [vp, vp, sz, vp, sz, vp, vp]
+        L.zntt_fri_domain_fill.argtypes = [i, ctypes.c_uint32, vp, vp]
+        L.zntt_fri_fold_device.argtypes = [i, vp, ctypes.c_uint32, _U64P, vp, ctypes.c_uint32, vp]
         L.zntt_poly_mul.argtypes = [i, _U64P, sz, _U64P, sz, sz, _U64P, ctypes.POINTER(ctypes.c_int64)]
         L.zntt_autotune.argtypes = [i, ctypes.c_uint32, ctypes.c_uint32]
         L.zntt_tune_save.argtypes = [ctypes.c_char_p]
@@ -558,6 +560,19 @@ def poly_mul(F: Field, a: np.ndarray, b: np.ndarray, max_degree: int):
     _check(lib().zntt_poly_mul(F.id, pa, len(a), pb, len(b), max_degree, out.ctypes.data_as(_U64P),
                                ctypes.byref(deg)))
     return out, deg.value
+
+
+def fri_domain_fill(F: Field, log_n: int, d_out: int, stream: int = 0) -> None:
+    """Domain(F).fill (libs/fri/src/root.zig:155-166) into a device buffer of 2^log_n elements."""
+    _ensure_init()
+    _check(lib().zntt_fri_domain_fill(F.id, log_n, d_out, stream or None))
+
+
+def fri_fold(F: Field, d_layer: int, log_n: int, alpha, d_out: int, log_table: int = 0, stream: int = 0) -> None:
+    """One FRI fold round (libs/fri/src/root.zig:396-403) of a device layer of 2^log_n evaluations
+    into 2^(log_n - 1); `alpha` in the field's scalar form (4 Montgomery limbs, or [value, 0, 0, 0])."""
+    _ensure_init()
+    _check(lib().zntt_fri_fold_device(F.id, d_layer, log_n, _root(alpha), d_out, log_table, stream or None))
 
 
 def autotune(F: Field, log_n_min: int, log_n_max: int) -> None:

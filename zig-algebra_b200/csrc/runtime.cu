@@ -548,6 +548,7 @@ int zntt_shutdown(void) {
   cudaStreamSynchronize(c.stream);
   while (!c.all_tables.empty()) free_entry(c.all_tables.back());
   small_shutdown();
+  fri_shutdown();
   free_coset_tabs();
   c.regs.clear();
   c.pool.trim();

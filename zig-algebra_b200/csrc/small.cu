@@ -223,6 +223,32 @@ __global__ void small_scale_kernel(const uint64_t* __restrict__ in, uint64_t* __
     out[i] = SF::mul(f, __ldg(in + i));
 }
 
+// out[i] = c * base^i for i < count (< 2^30), from power tables of base in
+// twiddle form; c in twiddle form too.  mul(c_tw, v_tw) is the twiddle form of
+// the product; with c = canonical one (not twiddle form) it is canonical.
+template <class SF>
+__global__ void small_powers_kernel(const uint64_t* __restrict__ pw, uint64_t c, uint64_t* __restrict__ out,
+                                    uint64_t count) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t v = SF::mul(__ldg(pw + (i & 1023)), __ldg(pw + 1024 + ((i >> 10) & 1023)));
+    out[i] = SF::mul(c, SF::mul(v, __ldg(pw + 2048 + (i >> 20))));
+  }
+}
+
+// One FRI fold round (libs/fri/src/root.zig:396-403) on canonical values;
+// half_inv, alpha and the table g^-j / 2 are in twiddle form.
+template <class SF>
+__global__ void small_fri_fold_kernel(const uint64_t* __restrict__ in, uint64_t* __restrict__ out,
+                                      const uint64_t* __restrict__ tab, uint64_t half, uint32_t stride,
+                                      uint64_t half_inv, uint64_t alpha) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < half; j += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t a = __ldg(in + j), b = __ldg(in + j + half);
+    const uint64_t even = SF::mul(half_inv, SF::add(a, b));
+    const uint64_t odd = SF::mul(__ldg(tab + (j << stride)), SF::sub(a, b));
+    out[j] = SF::add(even, SF::mul(alpha, odd));
+  }
+}
+
 __global__ void small_bit_reverse_kernel(const uint64_t* __restrict__ src, uint64_t* __restrict__ dst,
                                          uint32_t log_n) {
   const uint64_t n = 1ull << log_n;
@@ -789,7 +815,109 @@ int small_ntt_device(const zntt_twiddles* tw, const uint64_t* d_src, uint64_t* d
   return small_run(t, d_src, d_dst, d_scratch, inverse, inverse, ninv, st);
 }
 
+namespace {
+
+std::map<std::pair<int, uint32_t>, uint64_t*>& small_fold_tables() {
+  static std::map<std::pair<int, uint32_t>, uint64_t*> t;
+  return t;
+}
+
+// c * base^i (i < count) on the device: in twiddle form when c is given in
+// twiddle form, canonical when c is the plain integer 1.
+int small_powers(int field, uint64_t base, uint64_t c, uint64_t* out, uint64_t count, cudaStream_t st) {
+  const SmallHost& H = small_host(field);
+  std::vector<uint64_t> pw(3 * 1024);
+  uint64_t step = base % H.p;
+  for (int t = 0; t < 3; t++) {
+    uint64_t cur = 1;
+    for (int i = 0; i < 1024; i++) {
+      pw[t * 1024 + i] = H.to_tw(cur);
+      cur = H.mul(cur, step);
+    }
+    step = H.pow(step, 1024);
+  }
+  void* d_pw = nullptr;
+  int rc = pool_get(pw.size() * 8, &d_pw);
+  if (rc) return rc;
+  cudaError_t ce = cudaMemcpyAsync(d_pw, pw.data(), pw.size() * 8, cudaMemcpyHostToDevice, st);
+  if (ce == cudaSuccess && count) {
+    if (field == kGoldilocksField)
+      small_powers_kernel<Goldilocks><<<grid_for(count), 256, 0, st>>>((const uint64_t*)d_pw, c, out, count);
+    else
+      small_powers_kernel<BabyBear><<<grid_for(count), 256, 0, st>>>((const uint64_t*)d_pw, c, out, count);
+    ce = cudaGetLastError();
+  }
+  cudaError_t ce2 = cudaStreamSynchronize(st);  // the power tables return to the pool
+  pool_put(d_pw, pw.size() * 8);
+  if (ce == cudaSuccess) ce = ce2;
+  if (ce != cudaSuccess) return cuda_fail(ce, "powers");
+  return ZNTT_OK;
+}
+
+}  // namespace
+
+int small_domain_fill(int field, uint32_t log_n, uint64_t* d_out, void* stream) {
+  const SmallHost& H = small_host(field);
+  if (log_n > H.two_adicity) return set_error(ZNTT_ERR_ORDER_TOO_LARGE, "domain larger than the two-adicity (Domain.init)");
+  if (log_n > 30) return set_error(ZNTT_ERR_OUT_OF_MEMORY, "domain larger than 2^30 elements");
+  Context& c = ctx();
+  if (c.device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  uint64_t g[4];
+  small_primitive_root(field, log_n, g);
+  return small_powers(field, g[0], 1, d_out, 1ull << log_n, stream ? (cudaStream_t)stream : c.stream);
+}
+
+int small_fri_fold(int field, const uint64_t* d_layer, uint32_t log_n, const uint64_t* alpha, uint64_t* d_out,
+                   uint32_t log_table, void* stream) {
+  const SmallHost& H = small_host(field);
+  if (log_table == 0) log_table = log_n;
+  if (log_n < 1 || log_n > log_table) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "a fold needs 1 <= log_n <= log_table");
+  if (log_table > H.two_adicity) return set_error(ZNTT_ERR_ORDER_TOO_LARGE, "domain larger than the two-adicity");
+  if (log_table > 31) return set_error(ZNTT_ERR_OUT_OF_MEMORY, "domain larger than 2^31 elements");
+  const uint64_t n = 1ull << log_n, half = n / 2;
+  const char* lo = reinterpret_cast<const char*>(d_layer);
+  const char* oo = reinterpret_cast<const char*>(d_out);
+  if (oo < lo + n * 8 && lo < oo + half * 8) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "fold output overlaps the layer");
+  Context& c = ctx();
+  if (c.device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  auto& tabs = small_fold_tables();
+  const auto key = std::make_pair(field, log_table);
+  uint64_t* tab = nullptr;
+  auto it = tabs.find(key);
+  const uint64_t half_inv = H.inv(2);
+  if (it != tabs.end()) {
+    tab = it->second;
+  } else {
+    uint64_t g[4];
+    small_primitive_root(field, log_table, g);
+    const uint64_t count = 1ull << (log_table - 1);
+    cudaError_t ce = cudaMalloc((void**)&tab, count * 8);
+    if (ce != cudaSuccess) return cuda_fail(ce, "fold table");
+    int rc = small_powers(field, H.inv(g[0]), H.to_tw(half_inv), tab, count, c.stream);
+    if (rc) {
+      cudaFree(tab);
+      return rc;
+    }
+    tabs[key] = tab;
+  }
+  cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+  const uint64_t hv = H.to_tw(half_inv), av = H.to_tw(alpha[0] % H.p);
+  const uint32_t stride = log_table - log_n;
+  if (field == kGoldilocksField)
+    small_fri_fold_kernel<Goldilocks><<<grid_for(half), 256, 0, st>>>(d_layer, d_out, tab, half, stride, hv, av);
+  else
+    small_fri_fold_kernel<BabyBear><<<grid_for(half), 256, 0, st>>>(d_layer, d_out, tab, half, stride, hv, av);
+  cudaError_t ce = cudaGetLastError();
+  if (ce != cudaSuccess) return cuda_fail(ce, "fri fold");
+  return ZNTT_OK;
+}
+
 void small_shutdown() {
+  for (auto& kv : small_fold_tables())
+    if (kv.second) cudaFree(kv.second);
+  small_fold_tables().clear();
   SmallState& s = small_state();
   while (!s.all.empty()) small_free_entry(s.all.back());
   s.regs.clear();

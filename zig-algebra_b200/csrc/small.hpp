@@ -26,6 +26,11 @@ int small_twiddles_acquire(int field, uint32_t log_n, const uint64_t* root, zntt
 int small_twiddles_release(zntt_twiddles* tw);
 int small_ntt_device(const zntt_twiddles* tw, const uint64_t* d_src, uint64_t* d_dst, uint64_t* d_scratch, int mode,
                      void* stream);
+int small_domain_fill(int field, uint32_t log_n, uint64_t* d_out, void* stream);
+int small_fri_fold(int field, const uint64_t* d_layer, uint32_t log_n, const uint64_t* alpha, uint64_t* d_out,
+                   uint32_t log_table, void* stream);
 void small_shutdown();
+// FRI fold tables of the 256-bit fields (fri.cu).
+void fri_shutdown();
 
 }  // namespace zntt
