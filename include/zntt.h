@@ -244,6 +244,17 @@ int zntt_fri_domain_fill(int field, uint32_t log_n, uint64_t* d_out, void* strea
 int zntt_fri_fold_device(int field, const uint64_t* d_layer, uint32_t log_n, const uint64_t alpha[4],
                          uint64_t* d_out, uint32_t log_table, void* stream);
 
+/* The commitment of one FRI layer of 2^log_n evaluations (proveOn's commit step):
+ * leaf j = BLAKE3(toBytes(f[j]) || toBytes(f[j + n/2])) (hashPair, libs/fri/src/root.zig:286-295;
+ * toBytes = the canonical value in ceil(bits/8) little-endian bytes), and the heap-ordered
+ * BLAKE3 Merkle tree of MerkleTree.initFromHashes (libs/merkle/src/merkle_tree.zig:146-180):
+ * d_nodes (2^log_n digests of 32 bytes, 16-byte aligned) receives node 0 = zero, node 1 = the
+ * root, node i = BLAKE3(node 2i || node 2i+1), node n/2 + j = leaf j.  When root_out is not
+ * null the root is copied there and the call waits for the stream; otherwise it is
+ * stream-ordered.  All four fields. */
+int zntt_fri_commit_layer(int field, const uint64_t* d_layer, uint32_t log_n, uint8_t* d_nodes,
+                          uint8_t* root_out, void* stream);
+
 /* ---- serving: a continuously batching request server ---------------------------
  * Requests carry pinned host buffers.  A worker thread admits them in FIFO
  * order while their device buffers fit the HBM budget, turns whatever is

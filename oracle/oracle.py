@@ -89,6 +89,8 @@ def load(path: str | None = None):
     lib.zo_poly_eval.argtypes = [i, _U64P, sz, _U64P, sz, _U64P, i]
     lib.zo_fri_domain_fill.argtypes = [i, sz, _U64P]
     lib.zo_fri_fold.argtypes = [i, _U64P, sz, _U64P, _U64P, i]
+    lib.zo_blake3.argtypes = [ctypes.c_char_p, sz, ctypes.c_char_p]
+    lib.zo_fri_commit_layer.argtypes = [i, _U64P, sz, ctypes.c_void_p, i]
     if path.endswith("liboracle.so"):
         _lib = lib
     return lib
@@ -294,3 +296,20 @@ def fri_fold(field: int, layer: np.ndarray, log_n: int, alpha: np.ndarray, worke
     st = load().zo_fri_fold(field, _p(np.ascontiguousarray(layer)), log_n, _p(a), _p(out), workers)
     assert st == OK, st
     return out
+
+
+def blake3(msg: bytes) -> bytes:
+    """BLAKE3-256 of a message of at most 1024 bytes."""
+    out = ctypes.create_string_buffer(32)
+    st = load().zo_blake3(msg, len(msg), out)
+    assert st == OK, st
+    return out.raw
+
+
+def fri_commit_layer(field: int, layer: np.ndarray, log_n: int, workers: int = 1) -> np.ndarray:
+    """The FRI layer commitment (hashPair leaves, heap-ordered BLAKE3 Merkle tree): a
+    (2^log_n, 32) uint8 array of node digests, row 1 the root, row 0 zero."""
+    nodes = np.zeros((1 << log_n, 32), dtype=np.uint8)
+    st = load().zo_fri_commit_layer(field, _p(np.ascontiguousarray(layer)), log_n, nodes.ctypes.data, workers)
+    assert st == OK, st
+    return nodes

@@ -23,6 +23,10 @@
 //   libs/poly/src/vector.zig:24-32,68-73   powers / hadamard (coset LDE composition)
 //   libs/poly/src/poly.zig:76-107,197-224  fromCoeffs / normalize / mul (schoolbook) / eval
 //   libs/fri/src/root.zig:133-166,396-403  Domain.init / at / fill and the proveOn fold round
+//   libs/fri/src/root.zig:286-295, libs/merkle/src/merkle_tree.zig:146-180
+//                                          hashPair and MerkleTree.initFromHashes (the layer
+//                                          commitment), over BLAKE3 restated from its
+//                                          published specification (single-chunk messages)
 //   libs/parallel/src/root.zig:45-79       parallelFor fork-join semantics (harness only)
 //
 // The reference is Zig 0.16 and cannot be compiled in this environment; the
@@ -1207,6 +1211,119 @@ int zo_fri_fold(int field, const uint64_t* layer, size_t log_n, const uint64_t* 
         F.mul(x, g, x);
       }
     });
+    return ZO_OK;
+  });
+}
+
+}  // extern "C"
+
+// ---- BLAKE3 (single chunk) and the FRI layer commitment -------------------------
+
+static const uint32_t kB3Iv[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
+                                  0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
+static const uint8_t kB3Perm[16] = {2, 6, 3, 10, 7, 0, 4, 13, 1, 11, 12, 5, 9, 14, 15, 8};
+
+static inline uint32_t rotr32(uint32_t x, int r) { return (x >> r) | (x << (32 - r)); }
+
+static void b3_compress(const uint32_t cv[8], const uint32_t block[16], uint64_t counter, uint32_t len,
+                        uint32_t flags, uint32_t out[8]) {
+  uint32_t v[16], m[16];
+  for (int i = 0; i < 8; i++) v[i] = cv[i];
+  for (int i = 0; i < 4; i++) v[8 + i] = kB3Iv[i];
+  v[12] = (uint32_t)counter;
+  v[13] = (uint32_t)(counter >> 32);
+  v[14] = len;
+  v[15] = flags;
+  for (int i = 0; i < 16; i++) m[i] = block[i];
+  auto g = [&](int a, int b, int c, int d, uint32_t x, uint32_t y) {
+    v[a] += v[b] + x;
+    v[d] = rotr32(v[d] ^ v[a], 16);
+    v[c] += v[d];
+    v[b] = rotr32(v[b] ^ v[c], 12);
+    v[a] += v[b] + y;
+    v[d] = rotr32(v[d] ^ v[a], 8);
+    v[c] += v[d];
+    v[b] = rotr32(v[b] ^ v[c], 7);
+  };
+  for (int r = 0; r < 7; r++) {
+    g(0, 4, 8, 12, m[0], m[1]);
+    g(1, 5, 9, 13, m[2], m[3]);
+    g(2, 6, 10, 14, m[4], m[5]);
+    g(3, 7, 11, 15, m[6], m[7]);
+    g(0, 5, 10, 15, m[8], m[9]);
+    g(1, 6, 11, 12, m[10], m[11]);
+    g(2, 7, 8, 13, m[12], m[13]);
+    g(3, 4, 9, 14, m[14], m[15]);
+    if (r < 6) {
+      uint32_t t[16];
+      for (int i = 0; i < 16; i++) t[i] = m[kB3Perm[i]];
+      std::memcpy(m, t, sizeof(m));
+    }
+  }
+  for (int i = 0; i < 8; i++) out[i] = v[i] ^ v[i + 8];
+}
+
+// BLAKE3-256 of a message of at most 1024 bytes (one chunk): blocks compressed
+// in order from the IV, the first flagged CHUNK_START (1), the last CHUNK_END |
+// ROOT (2 | 8).
+static void b3_hash(const uint8_t* msg, size_t len, uint8_t out[32]) {
+  uint32_t cv[8];
+  std::memcpy(cv, kB3Iv, sizeof(cv));
+  const size_t nblocks = len == 0 ? 1 : (len + 63) / 64;
+  for (size_t b = 0; b < nblocks; b++) {
+    uint8_t blk[64] = {0};
+    const size_t bl = std::min<size_t>(64, len - b * 64);
+    if (bl) std::memcpy(blk, msg + b * 64, bl);
+    uint32_t words[16];
+    for (int i = 0; i < 16; i++)
+      words[i] = (uint32_t)blk[4 * i] | ((uint32_t)blk[4 * i + 1] << 8) | ((uint32_t)blk[4 * i + 2] << 16) |
+                 ((uint32_t)blk[4 * i + 3] << 24);
+    const uint32_t flags = (b == 0 ? 1u : 0u) | (b + 1 == nblocks ? 10u : 0u);
+    b3_compress(cv, words, 0, (uint32_t)bl, flags, cv);
+  }
+  for (int i = 0; i < 8; i++)
+    for (int k = 0; k < 4; k++) out[4 * i + k] = (uint8_t)(cv[i] >> (8 * k));
+}
+
+extern "C" {
+
+int zo_blake3(const uint8_t* msg, size_t len, uint8_t* out) {
+  if (len > 1024) return ZO_LENGTH_MISMATCH;
+  b3_hash(msg, len, out);
+  return ZO_OK;
+}
+
+// The commitment of one FRI layer (2^log_n slots): leaf j = BLAKE3(toBytes(f_j) ||
+// toBytes(f_{j+n/2})) with toBytes the canonical value in NUM_BYTES little-endian
+// bytes (libs/field/src/field.zig:244-252, 1002-1017), then the heap-ordered tree
+// of initFromHashes: nodes[h + j] = leaf j, nodes[i] = BLAKE3(nodes[2i] ||
+// nodes[2i+1]), h = n/2 (a power of two, so no padding).  `nodes` receives 2h
+// digests, nodes[0] zero.
+int zo_fri_commit_layer(int field, const uint64_t* layer, size_t log_n, uint8_t* nodes, int workers) {
+  return dispatch(field, [&](const auto& F) -> int {
+    constexpr int N = sizeof(F.P) / sizeof(uint64_t);
+    if (log_n < 1) return ZO_LOG_TOO_LARGE;
+    const size_t nb = (size_t)(F.BITS + 7) / 8, h = (size_t)1 << (log_n - 1);
+    std::memset(nodes, 0, 32);
+    auto bytes_of = [&](const uint64_t* slot, uint8_t* out) {
+      uint64_t m[N], c[N];
+      load<N>(slot, m);
+      F.from_mont(m, c);
+      for (size_t k = 0; k < nb; k++) out[k] = (uint8_t)(c[k / 8] >> (8 * (k % 8)));
+    };
+    parallel_for(h, workers, [&](size_t lo, size_t hi) {
+      for (size_t j = lo; j < hi; j++) {
+        uint8_t msg[64];
+        bytes_of(layer + 4 * j, msg);
+        bytes_of(layer + 4 * (j + h), msg + nb);
+        b3_hash(msg, 2 * nb, nodes + 32 * (h + j));
+      }
+    });
+    for (size_t w = h / 2; w >= 1; w /= 2) {
+      parallel_for(w, w >= 4096 ? workers : 1, [&](size_t lo, size_t hi) {
+        for (size_t i = w + lo; i < w + hi; i++) b3_hash(nodes + 32 * (2 * i), 64, nodes + 32 * i);
+      });
+    }
     return ZO_OK;
   });
 }

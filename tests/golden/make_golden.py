@@ -17,6 +17,9 @@ Two kinds of fixture:
      checked against the definition (n = 2^12, the plain 2^12 BN254-Fr case).
    * coset_lde.json -- a small blowup-4 coset extension over BLS12-381-Fr with
      shift 5, the reference's quadratic non-residue.
+   * fri_commit.json -- the reference's BLAKE3 known answer (libs/hash/src/root.zig,
+     kat.blake3_hello_world, copied as data) and FRI layer commitments (hashPair
+     leaves and the Merkle node array) of seeded layers over all four fields.
    * poly_mul.json -- polynomial products by the schoolbook sum over both
      fields: seeded factors of several lengths, trailing zero coefficients
      (normalized away), a zero factor, constants, and max_degree cases that
@@ -164,6 +167,35 @@ def poly_cases() -> list[dict]:
     return out
 
 
+def parse_blake3_kat(ref: str) -> dict:
+    path = os.path.join(ref, "libs/hash/src/root.zig")
+    text = open(path).read()
+    start = text.index("pub const blake3_hello_world")
+    body = text[start:text.index("};", start)]
+    lineno = text[:start].count("\n") + 1
+    digest = bytes(int(b, 16) for b in re.findall(r"0x([0-9a-f]{2})", body))
+    assert len(digest) == 32
+    return {"message": "hello world", "blake3": digest.hex(), "source": f"libs/hash/src/root.zig:{lineno}"}
+
+
+def fri_commit_cases(ref: str) -> dict:
+    kat = parse_blake3_kat(ref)
+    assert pyref.blake3(kat["message"].encode()).hex() == kat["blake3"]
+    fields = [("bn254_fr", pyref.BN254_FR_P, 32), ("bls12_381_fr", pyref.BLS12_381_FR_P, 32),
+              ("goldilocks", 0xFFFFFFFF00000001, 8), ("babybear", 0x78000001, 4)]
+    cases = []
+    for q, (name, p, nb) in enumerate(fields):
+        for log_n in (1, 2, 5, 8):
+            values = pyref.random_field_values(p, 1000 + 10 * q + log_n, 1 << log_n)
+            nodes = pyref.fri_commit_layer(values, nb)
+            case = {"field": name, "log_n": log_n, "num_bytes": nb, "values": [hex(v) for v in values],
+                    "root": nodes[1].hex()}
+            if log_n <= 5:  # the whole node array for the small layers, the root for the others
+                case["nodes"] = [x.hex() for x in nodes[1:]]
+            cases.append(case)
+    return {"kat": kat, "empty": pyref.blake3(b"").hex(), "cases": cases}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -173,6 +205,7 @@ def main() -> None:
     json.dump(fr_cases(), open(os.path.join(HERE, "fr_transforms.json"), "w"), indent=1)
     json.dump(lde_case(), open(os.path.join(HERE, "coset_lde.json"), "w"), indent=1)
     json.dump(poly_cases(), open(os.path.join(HERE, "poly_mul.json"), "w"), indent=1)
+    json.dump(fri_commit_cases(args.reference), open(os.path.join(HERE, "fri_commit.json"), "w"), indent=1)
     print("fixtures written to", HERE)
 
 

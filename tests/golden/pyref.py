@@ -13,6 +13,9 @@ the three is evidence rather than self-consistency:
 * Polynomial products by the schoolbook sum c_k = sum_{i+j=k} a_i b_j over
   Python integers (what Polynomial.mul of libs/poly/src/poly.zig:197-212
   computes), with the reference's degree convention (-1 for zero).
+* BLAKE3 (the published specification; single-chunk messages, up to 1024 bytes)
+  for the FRI layer commitment: hashPair (libs/fri/src/root.zig:286-295) and the
+  heap-ordered Merkle tree of libs/merkle/src/merkle_tree.zig:146-180.
 * Roots of unity as the reference derives them (libs/field/src/roots.zig:149-158):
   z = the first quadratic non-residue counting up from 2, raised to
   odd_part << (two_adicity - log_n).
@@ -163,3 +166,78 @@ def poly_mul(a: list[int], b: list[int], p: int) -> list[int]:
         for j in range(db + 1):
             c[i + j] = (c[i + j] + a[i] * b[j]) % p
     return c
+
+
+# ---- BLAKE3, single chunk ---------------------------------------------------------
+B3_IV = [0x6A09E667, 0xBB67AE85, 0x3C6EF372, 0xA54FF53A, 0x510E527F, 0x9B05688C, 0x1F83D9AB, 0x5BE0CD19]
+B3_PERM = [2, 6, 3, 10, 7, 0, 4, 13, 1, 11, 12, 5, 9, 14, 15, 8]
+B3_CHUNK_START, B3_CHUNK_END, B3_ROOT = 1, 2, 8
+
+
+def _rotr(x: int, r: int) -> int:
+    return ((x >> r) | (x << (32 - r))) & MASK32
+
+
+def _b3_compress(cv, block_words, counter, block_len, flags):
+    v = list(cv) + B3_IV[:4] + [counter & MASK32, counter >> 32, block_len, flags]
+    m = list(block_words)
+
+    def g(a, b, c, d, x, y):
+        v[a] = (v[a] + v[b] + x) & MASK32
+        v[d] = _rotr(v[d] ^ v[a], 16)
+        v[c] = (v[c] + v[d]) & MASK32
+        v[b] = _rotr(v[b] ^ v[c], 12)
+        v[a] = (v[a] + v[b] + y) & MASK32
+        v[d] = _rotr(v[d] ^ v[a], 8)
+        v[c] = (v[c] + v[d]) & MASK32
+        v[b] = _rotr(v[b] ^ v[c], 7)
+
+    for rnd in range(7):
+        g(0, 4, 8, 12, m[0], m[1])
+        g(1, 5, 9, 13, m[2], m[3])
+        g(2, 6, 10, 14, m[4], m[5])
+        g(3, 7, 11, 15, m[6], m[7])
+        g(0, 5, 10, 15, m[8], m[9])
+        g(1, 6, 11, 12, m[10], m[11])
+        g(2, 7, 8, 13, m[12], m[13])
+        g(3, 4, 9, 14, m[14], m[15])
+        if rnd < 6:
+            m = [m[i] for i in B3_PERM]
+    return [v[i] ^ v[i + 8] for i in range(8)]
+
+
+def blake3(msg: bytes) -> bytes:
+    """BLAKE3-256 of a message of at most one chunk (1024 bytes): its 64-byte blocks are
+    compressed in order from the IV, the first flagged CHUNK_START, the last CHUNK_END | ROOT."""
+    assert len(msg) <= 1024
+    blocks = [msg[i:i + 64] for i in range(0, len(msg), 64)] or [b""]
+    cv = B3_IV
+    for i, blk in enumerate(blocks):
+        words = [int.from_bytes((blk + bytes(64 - len(blk)))[4 * k:4 * k + 4], "little") for k in range(16)]
+        flags = (B3_CHUNK_START if i == 0 else 0) | (B3_CHUNK_END | B3_ROOT if i == len(blocks) - 1 else 0)
+        cv = _b3_compress(cv, words, 0, len(blk), flags)
+    return b"".join(w.to_bytes(4, "little") for w in cv)
+
+
+def to_bytes(value: int, num_bytes: int) -> bytes:
+    """Field.toBytes: the canonical value, little-endian, NUM_BYTES = ceil(bits / 8) bytes."""
+    return value.to_bytes(num_bytes, "little")
+
+
+def fri_commit_layer(values: list[int], num_bytes: int) -> list[bytes]:
+    """The FRI layer commitment of proveOn: leaf j = BLAKE3(toBytes(f_j) || toBytes(f_{j+n/2}))
+    (hashPair), then MerkleTree.initFromHashes: nodes[1] is the root, nodes[h + j] leaf j,
+    nodes[i] = BLAKE3(nodes[2i] || nodes[2i+1]); leaf counts are padded to a power of two with
+    BLAKE3 of the empty string.  Returns nodes[0 .. 2h) with nodes[0] all zero."""
+    half = len(values) // 2
+    h = 1
+    while h < half:
+        h *= 2
+    nodes = [bytes(32)] * (2 * h)
+    for j in range(half):
+        nodes[h + j] = blake3(to_bytes(values[j], num_bytes) + to_bytes(values[j + half], num_bytes))
+    for j in range(half, h):
+        nodes[h + j] = blake3(b"")
+    for i in range(h - 1, 0, -1):
+        nodes[i] = blake3(nodes[2 * i] + nodes[2 * i + 1])
+    return nodes

@@ -150,3 +150,41 @@ def test_fold_argument_errors(z):
         z.fri_fold(F, buf.data_ptr(), 5, one, buf[32:].data_ptr(), log_table=4)
     with pytest.raises(z.InvalidArgument):
         z.fri_fold(F, buf.data_ptr(), 0, one, buf[32:].data_ptr())
+
+
+def test_layer_commitment_matches_fixture_and_oracle(z):
+    """zntt_fri_commit_layer against the pure-Python fixture (roots and whole node arrays) and
+    the oracle at sizes that use the per-level launches and the one-CTA top levels."""
+    import json
+    torch = _torch()
+    d = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fri_commit.json")))
+    names = {F.name: (F, fid) for F, fid in _all(z)}
+    for c in d["cases"]:
+        F, fid = names[c["field"]]
+        slots = O.to_mont(fid, O.from_ints([int(v, 16) for v in c["values"]]))
+        dev = _to_dev(F, slots)
+        nodes = torch.zeros((1 << c["log_n"]) * 4, dtype=torch.int64, device="cuda")
+        root = z.fri_commit_layer(F, dev.data_ptr(), c["log_n"], nodes.data_ptr())
+        assert root.hex() == c["root"], (c["field"], c["log_n"])
+        if "nodes" in c:
+            got = nodes.cpu().numpy().view(np.uint8).reshape(-1, 32)
+            assert [x.tobytes().hex() for x in got[1:]] == c["nodes"]
+    for F, fid in _all(z):
+        for log_n in (12, 13, 16):
+            layer = O.random_elements(fid, 300 + log_n, 1 << log_n)
+            want = O.fri_commit_layer(fid, layer, log_n, workers=WORKERS)
+            nodes = torch.zeros((1 << log_n) * 4, dtype=torch.int64, device="cuda")
+            z.fri_commit_layer(F, _to_dev(F, layer).data_ptr(), log_n, nodes.data_ptr())
+            np.testing.assert_array_equal(nodes.cpu().numpy().view(np.uint8).reshape(-1, 32), want,
+                                          err_msg=f"{F.name} 2^{log_n}")
+
+
+def test_layer_commitment_full_size(z):
+    """A 2^24 Goldilocks layer and a 2^22 BN254-Fr layer against the oracle's root."""
+    torch = _torch()
+    for (F, fid), log_n in ((_all(z)[2], 24), (_all(z)[0], 22)):
+        layer = O.random_elements(fid, 400 + log_n, 1 << log_n)
+        want = O.fri_commit_layer(fid, layer, log_n, workers=WORKERS)
+        nodes = torch.empty((1 << log_n) * 4, dtype=torch.int64, device="cuda")
+        root = z.fri_commit_layer(F, _to_dev(F, layer).data_ptr(), log_n, nodes.data_ptr())
+        assert root == want[1].tobytes(), f"{F.name} 2^{log_n}"

@@ -306,3 +306,22 @@ def test_poly_mul_evaluates_to_the_product_of_evaluations():
         lhs = O.poly_eval(f, c1[:d + 1], x)
         rhs = O.elementwise(f, "mul", O.poly_eval(f, a, x), O.poly_eval(f, b, x))
         np.testing.assert_array_equal(lhs, rhs)
+
+
+def test_blake3_and_fri_commitment_fixture():
+    """BLAKE3 against the reference's own known answer (libs/hash/src/root.zig, kat) and the
+    FRI layer commitment (hashPair + MerkleTree.initFromHashes) against the pure-Python one,
+    on all four fields."""
+    d = json.load(open(os.path.join(GOLDEN, "fri_commit.json")))
+    assert O.blake3(d["kat"]["message"].encode()).hex() == d["kat"]["blake3"], d["kat"]["source"]
+    assert pyref.blake3(d["kat"]["message"].encode()).hex() == d["kat"]["blake3"]
+    assert O.blake3(b"").hex() == d["empty"]
+    for m in (b"a" * 63, b"b" * 64, b"c" * 65, b"d" * 200, bytes(range(256)) * 4):
+        assert O.blake3(m) == pyref.blake3(m), len(m)
+    for c in d["cases"]:
+        f = FIELD_IDS[c["field"]]
+        layer = _mont_of(f, [int(v, 16) for v in c["values"]])
+        nodes = O.fri_commit_layer(f, layer, c["log_n"], workers=4)
+        assert nodes[1].tobytes().hex() == c["root"], (c["field"], c["log_n"])
+        if "nodes" in c:
+            assert [x.tobytes().hex() for x in nodes[1:]] == c["nodes"]

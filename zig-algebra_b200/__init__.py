@@ -212,6 +212,7 @@ def lib():
         L.zntt_poly_mul_device.argtypes = [vp, vp, sz, vp, sz, vp, vp]
         L.zntt_fri_domain_fill.argtypes = [i, ctypes.c_uint32, vp, vp]
         L.zntt_fri_fold_device.argtypes = [i, vp, ctypes.c_uint32, _U64P, vp, ctypes.c_uint32, vp]
+        L.zntt_fri_commit_layer.argtypes = [i, vp, ctypes.c_uint32, vp, ctypes.c_char_p, vp]
         L.zntt_poly_mul.argtypes = [i, _U64P, sz, _U64P, sz, sz, _U64P, ctypes.POINTER(ctypes.c_int64)]
         L.zntt_autotune.argtypes = [i, ctypes.c_uint32, ctypes.c_uint32]
         L.zntt_tune_save.argtypes = [ctypes.c_char_p]
@@ -573,6 +574,15 @@ def fri_fold(F: Field, d_layer: int, log_n: int, alpha, d_out: int, log_table: i
     into 2^(log_n - 1); `alpha` in the field's scalar form (4 Montgomery limbs, or [value, 0, 0, 0])."""
     _ensure_init()
     _check(lib().zntt_fri_fold_device(F.id, d_layer, log_n, _root(alpha), d_out, log_table, stream or None))
+
+
+def fri_commit_layer(F: Field, d_layer: int, log_n: int, d_nodes: int, stream: int = 0) -> bytes:
+    """The FRI layer commitment (hashPair leaves, heap-ordered BLAKE3 Merkle tree) of a device
+    layer of 2^log_n evaluations into d_nodes (2^log_n x 32 bytes); returns the root."""
+    _ensure_init()
+    root = ctypes.create_string_buffer(32)
+    _check(lib().zntt_fri_commit_layer(F.id, d_layer, log_n, d_nodes, root, stream or None))
+    return root.raw
 
 
 def autotune(F: Field, log_n_min: int, log_n_max: int) -> None:
