@@ -45,7 +45,6 @@ struct SmallHost {
   }
   uint64_t inv(uint64_t a) const { return pow(a, p - 2); }  // p prime; inv(0) = 0
   uint64_t to_tw(uint64_t w) const { return mul(w % p, r); }
-  uint64_t from_tw(uint64_t w) const { return mul(w, inv(r)); }
 };
 
 const SmallHost kGoldilocksHost{kGoldilocksField, Goldilocks::P, 32, 1};
