@@ -388,6 +388,50 @@ __device__ __forceinline__ fe fe_mul_merged(const fe& a, const fe& b) {
   return r;
 }
 
+// x * 2^-256 mod p: Montgomery form to the canonical value (REDC of x), the
+// merged-row product with multiplier one but no multiplier products -- eight
+// reduction rows, about half the products of fe_mul.  For x < p the value
+// stays below p + 1, so one conditional subtraction finishes.
+template <class F>
+__device__ __forceinline__ fe fe_from_mont(const fe& x) {
+  uint32_t T[9], U[9];
+#pragma unroll
+  for (int q = 0; q < 8; q++) T[q] = x.v[q];
+  T[8] = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const uint32_t m = T[0] * F::N0;
+    ZNTT_MADP8("+r", "%8", T[0], T[1], T[2], T[3], T[4], T[5], T[6], T[7], T[8], F::P0, F::P2, F::P4, F::P6, m);
+    asm("mul.lo.u32 %0, %8, %9;\n\t"
+        "mul.hi.u32 %1, %8, %9;\n\t"
+        "mul.lo.u32 %2, %8, %10;\n\t"
+        "mul.hi.u32 %3, %8, %10;\n\t"
+        "mul.lo.u32 %4, %8, %11;\n\t"
+        "mul.hi.u32 %5, %8, %11;\n\t"
+        "mul.lo.u32 %6, %8, %12;\n\t"
+        "mul.hi.u32 %7, %8, %12;"
+        : "=r"(U[0]), "=r"(U[1]), "=r"(U[2]), "=r"(U[3]), "=r"(U[4]), "=r"(U[5]), "=r"(U[6]), "=r"(U[7])
+        : "r"(m), "n"(F::P1), "n"(F::P3), "n"(F::P5), "n"(F::P7));
+    asm("add.cc.u32  %0, %0, %8;\n\t"
+        "addc.cc.u32 %1, %1, %9;\n\t"
+        "addc.cc.u32 %2, %2, %10;\n\t"
+        "addc.cc.u32 %3, %3, %11;\n\t"
+        "addc.cc.u32 %4, %4, %12;\n\t"
+        "addc.cc.u32 %5, %5, %13;\n\t"
+        "addc.cc.u32 %6, %6, %14;\n\t"
+        "addc.u32    %7, %7, %15;"
+        : "+r"(T[1]), "+r"(T[2]), "+r"(T[3]), "+r"(T[4]), "+r"(T[5]), "+r"(T[6]), "+r"(T[7]), "+r"(T[8])
+        : "r"(U[0]), "r"(U[1]), "r"(U[2]), "r"(U[3]), "r"(U[4]), "r"(U[5]), "r"(U[6]), "r"(U[7]));
+#pragma unroll
+    for (int k = 0; k < 8; k++) T[k] = T[k + 1];
+    T[8] = 0;
+  }
+  fe r;
+#pragma unroll
+  for (int q = 0; q < 8; q++) r.v[q] = T[q];
+  return fe_reduce<F>(r);
+}
+
 // ---- split accumulators ----
 
 // Reduction of one row: add m * p with m = A0 * N0, which zeroes the low word

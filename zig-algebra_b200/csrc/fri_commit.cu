@@ -82,15 +82,12 @@ __device__ __forceinline__ void store_digest(uint4* nodes, uint64_t i, const uin
 }
 
 // Leaves of a 256-bit field: the canonical value is the Montgomery limbs times
-// 2^-256, i.e. a product with the integer one.
+// 2^-256 (fe_from_mont).
 template <class F>
 __global__ void leaf_kernel_wide(const uint4* __restrict__ layer, uint4* __restrict__ nodes, uint64_t h) {
   for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < h; j += (uint64_t)gridDim.x * blockDim.x) {
-    fe unit;
-#pragma unroll
-    for (int q = 0; q < 8; q++) unit.v[q] = q == 0 ? 1u : 0u;
-    const fe a = fe_mul<F>(fe_load_nc(layer + 2 * j), unit);
-    const fe b = fe_mul<F>(fe_load_nc(layer + 2 * (j + h)), unit);
+    const fe a = fe_from_mont<F>(fe_load_nc(layer + 2 * j));
+    const fe b = fe_from_mont<F>(fe_load_nc(layer + 2 * (j + h)));
     uint32_t m[16], d[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
