@@ -357,7 +357,9 @@ def run_zntt(args, rank, world, local):
     traffic = read_traffic(log_n)
     tw.close()
     extra = {}
-    if not args.headline_only:
+    # The configurations beside the headline run once, on rank 0 (the other ranks wait at the
+    # closing barrier, well inside its timeout): they describe the library, not the scaling.
+    if not args.headline_only and rank == 0:
         with torch.cuda.stream(stream):
             extra["batched"] = run_batched_config(z, torch, stream, steps=20, warmup=3)
             extra["coset_lde"] = run_lde_config(z, torch, stream, steps=5, warmup=2)
