@@ -1,17 +1,22 @@
 """Benchmark: BN254-Fr forward NTT of 2^24 elements on B200, one JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl zntt|reference] [--log-n L]
+                    [--headline-only] [--workload ntt|batched|lde|poly|small|fri|serve]
 
 A step is one forward transform (zig-ntt nttWithTwiddles semantics,
 libs/ntt/src/root.zig:148-175) of 2^24 seeded uniform BN254-Fr elements with
 the twiddle table resident on the device.  `value` is elements/s over all
 ranks with the input already in HBM (512 MiB per vector, larger than the
 126 MB L2, so no flush is needed between steps).  `e2e` is the same metric
-through the C ABI's host-buffer entry point zntt_ntt_with_twiddles, whose
-timed call includes the host->device copy of the input from pinned memory and
-the device->host copy of the result.  Under torchrun every rank transforms its
-own vector (independent objects: weak scaling, no collective on the data
-path); the time is the max over ranks.
+through the C ABI's host-buffer entry points: zntt_ntt_host_many over pinned
+host vectors, whose timed region includes every step's host->device copy of
+the input and device->host copy of the result (overlapped across vectors), and
+beside it one synchronous zntt_ntt_with_twiddles call.  Under torchrun every
+rank transforms its own vector (independent objects: weak scaling, no
+collective on the data path); the time is the max over ranks.  The default run
+adds, on rank 0, one key per configuration beside the headline (batched,
+coset_lde, poly_mul, small_fields, fri_fold); --workload prints one of them
+alone as its own line, and `serve` replays the request trace.
 
 `--impl reference` times the CPU restatement of zig-ntt (oracle/) on all host
 cores instead: zig-ntt has no GPU path and its toolchain (Zig 0.16) is not
