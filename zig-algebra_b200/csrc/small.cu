@@ -213,13 +213,14 @@ __global__ void small_twiddle_kernel(const uint64_t* __restrict__ pw, uint64_t* 
   }
 }
 
-// out[i] = in[i] * f (twiddle form in, f chosen by the caller): converts
-// between canonical and twiddle form (f = R^2 mod p, or canonical 1).
+// out[i] = in[i] * f (f chosen by the caller): converts between canonical and
+// twiddle form (f = R^2 mod p, or the integer 1).  in and out may be the same
+// array (each element is read, then written, by one thread), so the pointers
+// are not restrict and the loads are coherent.
 template <class SF>
-__global__ void small_scale_kernel(const uint64_t* __restrict__ in, uint64_t* __restrict__ out, uint64_t count,
-                                   uint64_t f) {
+__global__ void small_scale_kernel(const uint64_t* in, uint64_t* out, uint64_t count, uint64_t f) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x)
-    out[i] = SF::mul(f, __ldg(in + i));
+    out[i] = SF::mul(f, in[i]);
 }
 
 // out[i] = c * base^i for i < count (< 2^30), from power tables of base in
