@@ -353,3 +353,27 @@ def test_pipelined_host_vectors_match_single_calls(z, log_n):
         for b, w in zip(bufs, wants):
             np.testing.assert_array_equal(b.numpy().view(np.uint64).reshape(-1, 4), w)
         z.freeTwiddles(F, tw_host)
+
+
+def test_largest_order_transform(z):
+    """BN254-Fr at its two-adicity, 2^28 (8 GiB per vector; the plan's later passes have tile
+    rows of one element): inverse(forward(x)) == x, and forward outputs at sampled indices equal
+    the definition sum_j x_j w^(jk)."""
+    torch = _torch()
+    F = z.BN254_FR
+    log_n = F.two_adicity
+    n = 1 << log_n
+    x = torch.empty(n * 4, dtype=torch.int64, device="cuda")
+    z.random_elements(F, 2828, x.data_ptr(), n)
+    root = z.primitiveRootOfUnity(F, log_n)
+    X = torch.empty_like(x)
+    with z.DeviceTwiddles(F, log_n, root) as tw:
+        z.ntt_device(tw, x.data_ptr(), X.data_ptr(), z.FORWARD)
+        back = torch.empty_like(x)
+        z.ntt_device(tw, X.data_ptr(), back.data_ptr(), z.INVERSE)
+        torch.cuda.synchronize()
+        assert torch.equal(back, x)
+        del back
+    ks = [0, 1, n // 2 + 7, n - 1]
+    pts = O.dft_points(F.id, _to_host(x), root, ks, workers=WORKERS)
+    np.testing.assert_array_equal(_to_host(X)[ks], pts)
