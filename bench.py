@@ -658,6 +658,7 @@ def run_fri_config(z, torch, stream, steps, warmup, log_n=24):
     sptr = stream.cuda_stream
     peaks, hbm_src = measured_peaks()
     hbm_peak = float(peaks["hbm_gbs"])
+    b3_peak = z.probe_blake3()
     out = {"workload": f"FRI fold of a 2^{log_n}-evaluation layer, the chain 2^{log_n} -> 2^10, and the "
                        f"layer's BLAKE3 Merkle commitment",
            "fields": {}}
@@ -698,6 +699,9 @@ def run_fri_config(z, torch, stream, steps, warmup, log_n=24):
                     "frac": moved / (ms_one * 1e-3) / 1e9 / hbm_peak, "peak_source": hbm_src},
             "chain_rounds": log_n - 10, "chain_ms": ms_chain,
             "commit_ms": ms_commit, "commit_hashes_per_s": (n - 1) / (ms_commit * 1e-3),
+            "commit_roofline": {"bound": "alu", "achieved": (n - 1) / (ms_commit * 1e-3), "peak": b3_peak,
+                                "unit": "compressions/s", "frac": (n - 1) / (ms_commit * 1e-3) / b3_peak,
+                                "peak_source": "zntt_probe_blake3: chained compressions in registers"},
             "commit_note": "hashPair leaves + BLAKE3 Merkle tree, n - 1 single-block compressions; "
                            "the call copies the root to the host, inside the timed region",
         }

@@ -348,6 +348,10 @@ int zntt_probe_imad(double* imad_per_second);
 /* 32x32->64 multiply-adds (mad.wide.u32) per second: one 8x32-bit CIOS
  * product needs 2*8*8 + 8 = 136 of them, so this / 136 is the modmul ceiling. */
 int zntt_probe_mul_wide(double* products_per_second);
+/* Single-block BLAKE3 compressions per second, chained in registers with the
+ * instruction mix of the commitment's node levels and no memory traffic: the
+ * roofline of zntt_fri_commit_layer, which makes n - 1 compressions. */
+int zntt_probe_blake3(double* compressions_per_second);
 int zntt_probe_modmul(int field, double* modmul_per_second);
 
 #ifdef __cplusplus

@@ -154,7 +154,9 @@ def test_fold_argument_errors(z):
 
 def test_layer_commitment_matches_fixture_and_oracle(z):
     """zntt_fri_commit_layer against the pure-Python fixture (roots and whole node arrays) and
-    the oracle at sizes that use the per-level launches and the one-CTA top levels."""
+    the oracle's whole node arrays at sizes on both sides of each launch boundary: leaves alone
+    below 2^10 evaluations, one subtree launch, chained subtree launches, and the one-CTA top
+    levels."""
     import json
     torch = _torch()
     d = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fri_commit.json")))
@@ -170,7 +172,7 @@ def test_layer_commitment_matches_fixture_and_oracle(z):
             got = nodes.cpu().numpy().view(np.uint8).reshape(-1, 32)
             assert [x.tobytes().hex() for x in got[1:]] == c["nodes"]
     for F, fid in _all(z):
-        for log_n in (12, 13, 16):
+        for log_n in (9, 10, 12, 13, 14, 16, 18):
             layer = O.random_elements(fid, 300 + log_n, 1 << log_n)
             want = O.fri_commit_layer(fid, layer, log_n, workers=WORKERS)
             nodes = torch.zeros((1 << log_n) * 4, dtype=torch.int64, device="cuda")
@@ -188,3 +190,9 @@ def test_layer_commitment_full_size(z):
         nodes = torch.empty((1 << log_n) * 4, dtype=torch.int64, device="cuda")
         root = z.fri_commit_layer(F, _to_dev(F, layer).data_ptr(), log_n, nodes.data_ptr())
         assert root == want[1].tobytes(), f"{F.name} 2^{log_n}"
+
+
+def test_blake3_probe(z):
+    """The commitment's roofline probe runs and gives a plausible compression rate."""
+    rate = z.probe_blake3()
+    assert 1e9 < rate < 1e13

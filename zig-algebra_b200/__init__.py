@@ -200,6 +200,7 @@ def lib():
         L.zntt_probe_imad.argtypes = [ctypes.POINTER(ctypes.c_double)]
         L.zntt_probe_modmul.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
         L.zntt_probe_mul_wide.argtypes = [ctypes.POINTER(ctypes.c_double)]
+        L.zntt_probe_blake3.argtypes = [ctypes.POINTER(ctypes.c_double)]
         L.zntt_ntt_device_inplace_noalloc.argtypes = [vp, vp, i, vp]
         L.zntt_batch_create.argtypes = [i, ctypes.POINTER(Job), sz, i, ctypes.POINTER(vp)]
         L.zntt_batch_run.argtypes = [vp, vp]
@@ -465,6 +466,14 @@ def probe_mul_wide() -> float:
     _ensure_init()
     v = ctypes.c_double()
     _check(lib().zntt_probe_mul_wide(ctypes.byref(v)))
+    return v.value
+
+
+def probe_blake3() -> float:
+    """Single-block BLAKE3 compressions per second in registers (the commitment's roofline)."""
+    _ensure_init()
+    v = ctypes.c_double()
+    _check(lib().zntt_probe_blake3(ctypes.byref(v)))
     return v.value
 
 

@@ -11,8 +11,14 @@
 // Goldilocks, 4 for BabyBear).  The node array is the reference's heap order:
 // node 1 the root, node h + j leaf j (h = n/2), node i the hash of nodes 2i
 // and 2i + 1; node 0 is zero.
+//
+// The tree is built bottom-up in subtrees: a thread hashes two siblings and
+// their parent in registers, and a CTA of 256 threads takes its 256 parents
+// three levels further through shared memory, where every level still fills
+// whole warps.  One launch therefore writes five levels of the tree.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 
 #include "field.cuh"
@@ -23,23 +29,56 @@ namespace zntt {
 
 namespace {
 
+constexpr int kThreads = 256;     // CTA size of the subtree kernels
+constexpr int kSharedLevels = 3;  // levels a CTA builds in shared memory (256 -> 32 nodes)
+// The 256-bit fields' leaves keep BLAKE3's adds on the ALU (b3_g below).
+constexpr bool kWideLeafMulAdd = false;
+
 __device__ __forceinline__ uint32_t rotr(uint32_t x, int r) { return __funnelshift_r(x, x, r); }
 
-__device__ __forceinline__ void b3_g(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& d, uint32_t x, uint32_t y) {
-  a = a + b + x;
-  d = rotr(d ^ a, 16);
-  c = c + d;
-  b = rotr(b ^ c, 12);
-  a = a + b + y;
-  d = rotr(d ^ a, 8);
-  c = c + d;
-  b = rotr(b ^ c, 7);
+// x + y as a multiply-add by `one`, a kernel argument equal to 1 that the
+// compiler cannot fold: the add then issues on the multiply-add pipe instead
+// of the integer ALU, which the XORs and rotations keep busy.
+__device__ __forceinline__ uint32_t madd(uint32_t x, uint32_t one, uint32_t y) {
+  uint32_t r;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(one), "r"(y));
+  return r;
+}
+
+// BLAKE3's quarter-round G.  kMulAdd puts its six adds on the multiply-add
+// pipe (the node levels and the small fields' leaves, where that pipe is
+// otherwise idle); without it they stay on the ALU (the 256-bit fields'
+// leaves, whose Montgomery conversions load the multiply pipe).
+template <bool kMulAdd>
+__device__ __forceinline__ void b3_g(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t& d, uint32_t x, uint32_t y,
+                                     uint32_t one) {
+  if constexpr (kMulAdd) {
+    a = madd(b, one, madd(x, one, a));
+    d = rotr(d ^ a, 16);
+    c = madd(d, one, c);
+    b = rotr(b ^ c, 12);
+    a = madd(b, one, madd(y, one, a));
+    d = rotr(d ^ a, 8);
+    c = madd(d, one, c);
+    b = rotr(b ^ c, 7);
+  } else {
+    a = a + b + x;
+    d = rotr(d ^ a, 16);
+    c = c + d;
+    b = rotr(b ^ c, 12);
+    a = a + b + y;
+    d = rotr(d ^ a, 8);
+    c = c + d;
+    b = rotr(b ^ c, 7);
+  }
 }
 
 // BLAKE3 of one block of `len` bytes (m, zero beyond len) as a whole message:
 // 7 rounds of the G mixes, the message words permuted between rounds, output
 // words 0..7 of state XOR state words 8..15.
-__device__ __forceinline__ void b3_hash_block(const uint32_t (&msg)[16], uint32_t len, uint32_t (&out)[8]) {
+template <bool kMulAdd>
+__device__ __forceinline__ void b3_hash_block(const uint32_t (&msg)[16], uint32_t len, uint32_t (&out)[8],
+                                              uint32_t one) {
   constexpr uint32_t IV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
                               0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
   constexpr int PERM[16] = {2, 6, 3, 10, 7, 0, 4, 13, 1, 11, 12, 5, 9, 14, 15, 8};
@@ -56,14 +95,14 @@ __device__ __forceinline__ void b3_hash_block(const uint32_t (&msg)[16], uint32_
   for (int i = 0; i < 16; i++) m[i] = msg[i];
 #pragma unroll
   for (int r = 0; r < 7; r++) {
-    b3_g(v[0], v[4], v[8], v[12], m[0], m[1]);
-    b3_g(v[1], v[5], v[9], v[13], m[2], m[3]);
-    b3_g(v[2], v[6], v[10], v[14], m[4], m[5]);
-    b3_g(v[3], v[7], v[11], v[15], m[6], m[7]);
-    b3_g(v[0], v[5], v[10], v[15], m[8], m[9]);
-    b3_g(v[1], v[6], v[11], v[12], m[10], m[11]);
-    b3_g(v[2], v[7], v[8], v[13], m[12], m[13]);
-    b3_g(v[3], v[4], v[9], v[14], m[14], m[15]);
+    b3_g<kMulAdd>(v[0], v[4], v[8], v[12], m[0], m[1], one);
+    b3_g<kMulAdd>(v[1], v[5], v[9], v[13], m[2], m[3], one);
+    b3_g<kMulAdd>(v[2], v[6], v[10], v[14], m[4], m[5], one);
+    b3_g<kMulAdd>(v[3], v[7], v[11], v[15], m[6], m[7], one);
+    b3_g<kMulAdd>(v[0], v[5], v[10], v[15], m[8], m[9], one);
+    b3_g<kMulAdd>(v[1], v[6], v[11], v[12], m[10], m[11], one);
+    b3_g<kMulAdd>(v[2], v[7], v[8], v[13], m[12], m[13], one);
+    b3_g<kMulAdd>(v[3], v[4], v[9], v[14], m[14], m[15], one);
     if (r < 6) {
       uint32_t t[16];
 #pragma unroll
@@ -76,76 +115,205 @@ __device__ __forceinline__ void b3_hash_block(const uint32_t (&msg)[16], uint32_
   for (int i = 0; i < 8; i++) out[i] = v[i] ^ v[i + 8];
 }
 
+// The parent digest of two child digests.
+__device__ __forceinline__ void b3_parent(const uint32_t (&l)[8], const uint32_t (&r)[8], uint32_t (&out)[8],
+                                          uint32_t one) {
+  uint32_t m[16];
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    m[q] = l[q];
+    m[8 + q] = r[q];
+  }
+  b3_hash_block<true>(m, 64, out, one);
+}
+
 __device__ __forceinline__ void store_digest(uint4* nodes, uint64_t i, const uint32_t (&d)[8]) {
   nodes[2 * i] = make_uint4(d[0], d[1], d[2], d[3]);
   nodes[2 * i + 1] = make_uint4(d[4], d[5], d[6], d[7]);
 }
 
-// Leaves of a 256-bit field: the canonical value is the Montgomery limbs times
-// 2^-256 (fe_from_mont).
+__device__ __forceinline__ void load_digest(const uint4* nodes, uint64_t i, uint32_t (&d)[8]) {
+  const uint4 a = nodes[2 * i], b = nodes[2 * i + 1];
+  d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w;
+  d[4] = b.x; d[5] = b.y; d[6] = b.z; d[7] = b.w;
+}
+
+// hashPair leaf j of a 256-bit field: the canonical values of f_j and f_{j+h}
+// are the Montgomery limbs times 2^-256 (fe_from_mont).
 template <class F>
-__global__ void leaf_kernel_wide(const uint4* __restrict__ layer, uint4* __restrict__ nodes, uint64_t h) {
-  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < h; j += (uint64_t)gridDim.x * blockDim.x) {
-    const fe a = fe_from_mont<F>(fe_load_nc(layer + 2 * j));
-    const fe b = fe_from_mont<F>(fe_load_nc(layer + 2 * (j + h)));
-    uint32_t m[16], d[8];
+__device__ __forceinline__ void leaf_wide(const uint4* layer, uint64_t h, uint64_t j, uint32_t (&d)[8],
+                                          uint32_t one) {
+  const fe a = fe_from_mont<F>(fe_load_nc(layer + 2 * j));
+  const fe b = fe_from_mont<F>(fe_load_nc(layer + 2 * (j + h)));
+  uint32_t m[16];
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
-      m[q] = a.v[q];
-      m[8 + q] = b.v[q];
-    }
-    b3_hash_block(m, 64, d);
+  for (int q = 0; q < 8; q++) {
+    m[q] = a.v[q];
+    m[8 + q] = b.v[q];
+  }
+  b3_hash_block<kWideLeafMulAdd>(m, 64, d, one);
+}
+
+// hashPair leaf j of a small field: canonical u64 values, `nb` bytes each (8 or 4).
+__device__ __forceinline__ void leaf_small(const uint64_t* layer, uint64_t h, uint64_t j, uint32_t nb,
+                                           uint32_t (&d)[8], uint32_t one) {
+  const uint64_t a = __ldg(layer + j), b = __ldg(layer + j + h);
+  uint32_t m[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) m[q] = 0;
+  if (nb == 8) {
+    m[0] = (uint32_t)a;
+    m[1] = (uint32_t)(a >> 32);
+    m[2] = (uint32_t)b;
+    m[3] = (uint32_t)(b >> 32);
+  } else {
+    m[0] = (uint32_t)a;
+    m[1] = (uint32_t)b;
+  }
+  b3_hash_block<true>(m, 2 * nb, d, one);
+}
+
+// Source of a subtree's bottom level.  Leaf sources hash pairs of layer
+// values; the node source reads digests an earlier launch wrote.
+struct NodeSource {
+  const uint4* nodes;
+  uint64_t width;  // the level read: nodes [width, 2 width)
+  __device__ __forceinline__ void get(uint64_t j, uint32_t (&d)[8], uint32_t) const {
+    load_digest(nodes, width + j, d);
+  }
+};
+template <class F>
+struct WideLeafSource {
+  const uint4* layer;
+  uint64_t h;
+  __device__ __forceinline__ void get(uint64_t j, uint32_t (&d)[8], uint32_t one) const {
+    leaf_wide<F>(layer, h, j, d, one);
+  }
+};
+struct SmallLeafSource {
+  const uint64_t* layer;
+  uint64_t h;
+  uint32_t nb;
+  __device__ __forceinline__ void get(uint64_t j, uint32_t (&d)[8], uint32_t one) const {
+    leaf_small(layer, h, j, nb, d, one);
+  }
+};
+
+// Every leaf j < h on its own (small trees).
+template <class Src>
+__global__ void leaf_kernel(Src src, uint4* __restrict__ nodes, uint64_t h, uint32_t one) {
+  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < h; j += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t d[8];
+    src.get(j, d, one);
     store_digest(nodes, h + j, d);
   }
 }
 
-// Leaves of a small field: canonical u64 values, `nb` bytes each (8 or 4).
-__global__ void leaf_kernel_small(const uint64_t* __restrict__ layer, uint4* __restrict__ nodes, uint64_t h,
-                                  uint32_t nb) {
-  for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < h; j += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t a = __ldg(layer + j), b = __ldg(layer + j + h);
-    uint32_t m[16], d[8];
-#pragma unroll
-    for (int q = 0; q < 16; q++) m[q] = 0;
-    if (nb == 8) {
-      m[0] = (uint32_t)a;
-      m[1] = (uint32_t)(a >> 32);
-      m[2] = (uint32_t)b;
-      m[3] = (uint32_t)(b >> 32);
-    } else {
-      m[0] = (uint32_t)a;
-      m[1] = (uint32_t)b;
+// One subtree per CTA over the level of width w (a multiple of 512): thread t
+// takes entries 2u and 2u + 1 of that level (u = 256 b + t), hashes their
+// parent in registers, and the CTA builds three more levels in shared memory,
+// each still whole warps (128, 64, 32 nodes).  Writes the levels of width
+// w/2 .. w/16, and the bottom level itself when it is made here (leaves).
+template <class Src, bool kStoreBottom>
+__global__ void __launch_bounds__(kThreads) subtree_kernel(Src src, uint4* __restrict__ nodes, uint64_t w,
+                                                           uint32_t one) {
+  __shared__ uint4 buf_a[kThreads][2];
+  __shared__ uint4 buf_b[kThreads / 2][2];
+  const uint32_t t = threadIdx.x;
+  const uint64_t u = (uint64_t)blockIdx.x * kThreads + t;
+  uint32_t l[8], r[8], p[8];
+  src.get(2 * u, l, one);
+  if (kStoreBottom) store_digest(nodes, w + 2 * u, l);
+  src.get(2 * u + 1, r, one);
+  if (kStoreBottom) store_digest(nodes, w + 2 * u + 1, r);
+  b3_parent(l, r, p, one);
+  uint64_t wl = w >> 1;  // width of the level p belongs to
+  store_digest(nodes, wl + u, p);
+  buf_a[t][0] = make_uint4(p[0], p[1], p[2], p[3]);
+  buf_a[t][1] = make_uint4(p[4], p[5], p[6], p[7]);
+  __syncthreads();
+  uint4(*from)[2] = buf_a;
+  uint4(*to)[2] = buf_b;
+#pragma unroll 1
+  for (uint32_t lev = 1, cnt = kThreads / 2; lev <= kSharedLevels; lev++, cnt >>= 1) {
+    wl >>= 1;
+    if (t < cnt) {
+      const uint4 a0 = from[2 * t][0], a1 = from[2 * t][1], b0 = from[2 * t + 1][0], b1 = from[2 * t + 1][1];
+      const uint32_t m[16] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w,
+                              b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+      uint32_t d[8];
+      b3_hash_block<true>(m, 64, d, one);
+      store_digest(nodes, wl + (uint64_t)blockIdx.x * cnt + t, d);
+      if (lev < kSharedLevels) {
+        to[t][0] = make_uint4(d[0], d[1], d[2], d[3]);
+        to[t][1] = make_uint4(d[4], d[5], d[6], d[7]);
+      }
     }
-    b3_hash_block(m, 2 * nb, d);
-    store_digest(nodes, h + j, d);
+    __syncthreads();
+    uint4(*x)[2] = from;
+    from = to;
+    to = x;
   }
-}
-
-__device__ __forceinline__ void hash_node(uint4* nodes, uint64_t i) {
-  const uint4 c0 = nodes[4 * i], c1 = nodes[4 * i + 1], c2 = nodes[4 * i + 2], c3 = nodes[4 * i + 3];
-  const uint32_t m[16] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w,
-                          c2.x, c2.y, c2.z, c2.w, c3.x, c3.y, c3.z, c3.w};
-  uint32_t d[8];
-  b3_hash_block(m, 64, d);
-  store_digest(nodes, i, d);
-}
-
-// One level: nodes w .. 2w-1 from their children (nodes 2w .. 4w-1).
-__global__ void level_kernel(uint4* nodes, uint64_t w) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < w; i += (uint64_t)gridDim.x * blockDim.x)
-    hash_node(nodes, w + i);
 }
 
 // The levels of width w_top, w_top / 2, ..., 1 in one CTA; the barrier between
 // levels orders each level's global writes before the next level's reads.
-__global__ void top_levels_kernel(uint4* nodes, uint32_t w_top) {
+__global__ void top_levels_kernel(uint4* nodes, uint32_t w_top, uint32_t one) {
   for (uint32_t w = w_top; w >= 1; w >>= 1) {
-    for (uint32_t i = threadIdx.x; i < w; i += blockDim.x) hash_node(nodes, (uint64_t)w + i);
+    for (uint32_t i = threadIdx.x; i < w; i += blockDim.x) {
+      uint32_t l[8], r[8], d[8];
+      load_digest(nodes, 2 * ((uint64_t)w + i), l);
+      load_digest(nodes, 2 * ((uint64_t)w + i) + 1, r);
+      b3_parent(l, r, d, one);
+      store_digest(nodes, (uint64_t)w + i, d);
+    }
     __syncthreads();
   }
 }
 
+// Roofline probe: chained single-block compressions in registers, the node
+// levels' instruction mix with no memory traffic.  Each compression's message
+// starts with the previous digest, so none can be hoisted or skipped.
+__global__ void blake3_probe_kernel(uint32_t* sink, uint32_t iters, uint32_t one) {
+  uint32_t m[16], d[8];
+#pragma unroll
+  for (int q = 0; q < 16; q++) m[q] = threadIdx.x * 977u + blockIdx.x * 131u + q;
+  for (uint32_t it = 0; it < iters; it++) {
+    b3_hash_block<true>(m, 64, d, one);
+#pragma unroll
+    for (int q = 0; q < 8; q++) m[q] = d[q];
+  }
+  uint32_t x = 0;
+#pragma unroll
+  for (int q = 0; q < 8; q++) x ^= m[q];
+  if (x == 0x9e3779b9u) sink[0] = x;
+}
+
 int grid_for_count(uint64_t count) { return (int)std::min<uint64_t>((count + 255) / 256, 148 * 16); }
+
+// Leaves, then subtrees of five levels while a level has 512 entries or more,
+// then the rest in one CTA.
+template <class Src>
+cudaError_t build_tree(const Src& src, uint4* nodes, uint64_t h, cudaStream_t st) {
+  uint64_t w = h;
+  if (h >= 2 * kThreads) {
+    subtree_kernel<Src, true><<<(unsigned)(h / (2 * kThreads)), kThreads, 0, st>>>(src, nodes, h, 1u);
+    w = h >> (1 + kSharedLevels);
+  } else {
+    leaf_kernel<Src><<<grid_for_count(h), kThreads, 0, st>>>(src, nodes, h, 1u);
+  }
+  cudaError_t ce = cudaGetLastError();
+  for (; w >= 2 * kThreads && ce == cudaSuccess; w >>= 1 + kSharedLevels) {
+    subtree_kernel<NodeSource, false><<<(unsigned)(w / (2 * kThreads)), kThreads, 0, st>>>(NodeSource{nodes, w},
+                                                                                           nodes, w, 1u);
+    ce = cudaGetLastError();
+  }
+  if (w >= 2 && ce == cudaSuccess) {
+    top_levels_kernel<<<1, 1024, 0, st>>>(nodes, (uint32_t)(w / 2), 1u);
+    ce = cudaGetLastError();
+  }
+  return ce;
+}
 
 }  // namespace
 
@@ -175,29 +343,51 @@ extern "C" int zntt_fri_commit_layer(int field, const uint64_t* d_layer, uint32_
   uint4* nodes = reinterpret_cast<uint4*>(d_nodes);
   cudaError_t ce = cudaMemsetAsync(nodes, 0, 32, st);  // node 0 is unused and zero
   if (ce == cudaSuccess) {
+    const uint4* wide = reinterpret_cast<const uint4*>(d_layer);
     if (field == kBn254Fr)
-      leaf_kernel_wide<Bn254Fr><<<grid_for_count(h), 256, 0, st>>>(reinterpret_cast<const uint4*>(d_layer), nodes, h);
+      ce = build_tree(WideLeafSource<Bn254Fr>{wide, h}, nodes, h, st);
     else if (field == kBls12381Fr)
-      leaf_kernel_wide<Bls12381Fr><<<grid_for_count(h), 256, 0, st>>>(reinterpret_cast<const uint4*>(d_layer), nodes,
-                                                                        h);
+      ce = build_tree(WideLeafSource<Bls12381Fr>{wide, h}, nodes, h, st);
     else
-      leaf_kernel_small<<<grid_for_count(h), 256, 0, st>>>(d_layer, nodes, h, field == kGoldilocksField ? 8u : 4u);
-    ce = cudaGetLastError();
-  }
-  // Wide levels one launch each; the top 2^11 - 1 nodes in one CTA.
-  uint64_t w = h / 2;
-  for (; w > 2048 && ce == cudaSuccess; w /= 2) {
-    level_kernel<<<grid_for_count(w), 256, 0, st>>>(nodes, w);
-    ce = cudaGetLastError();
-  }
-  if (w >= 1 && ce == cudaSuccess) {
-    top_levels_kernel<<<1, 1024, 0, st>>>(nodes, (uint32_t)w);
-    ce = cudaGetLastError();
+      ce = build_tree(SmallLeafSource{d_layer, h, field == kGoldilocksField ? 8u : 4u}, nodes, h, st);
   }
   if (ce == cudaSuccess && root_out) {
     ce = cudaMemcpyAsync(root_out, d_nodes + 32, 32, cudaMemcpyDeviceToHost, st);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
   }
   if (ce != cudaSuccess) return cuda_fail(ce, "fri layer commitment");
+  return ZNTT_OK;
+}
+
+extern "C" int zntt_probe_blake3(double* per_second) {
+  clear_error();
+  if (!per_second) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
+  Context& c = ctx();
+  if (c.device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  int sms = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, blake3_probe_kernel, kThreads, 0);
+  const int blocks = sms * std::max(per_sm, 1);  // one full wave
+  const uint32_t iters = 2048;
+  void* sink = nullptr;
+  int rc = pool_get(64, &sink);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  blake3_probe_kernel<<<blocks, kThreads, 0, c.stream>>>((uint32_t*)sink, 64, 1u);  // warm-up
+  cudaEventRecord(e0, c.stream);
+  blake3_probe_kernel<<<blocks, kThreads, 0, c.stream>>>((uint32_t*)sink, iters, 1u);
+  cudaEventRecord(e1, c.stream);
+  cudaError_t ce = cudaGetLastError();
+  if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+  float ms = 0;
+  if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (ce == cudaSuccess) pool_put(sink, 64);  // the probe has finished with it
+  if (ce != cudaSuccess) return cuda_fail(ce, "blake3 probe");
+  *per_second = (double)blocks * kThreads * iters / (ms * 1e-3);
   return ZNTT_OK;
 }
