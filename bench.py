@@ -685,6 +685,29 @@ def run_fri_config(z, torch, stream, steps, warmup, log_n=24):
 
         nodes = torch.empty(n * 4, dtype=torch.int64, device="cuda")  # 2^log_n digests of 32 bytes
         commit = lambda: z.fri_commit_layer(F, layer.data_ptr(), log_n, nodes.data_ptr(), stream=sptr)  # noqa: E731
+        # proveOn's commit loop over the same buffers (a fixed alpha stands in for the caller's
+        # transcript) and 64 query openings from the resident layers and trees.
+        rounds = log_n - 10
+        players = [layer.data_ptr()] + [b.data_ptr() for b in bufs]
+        ptrees = [nodes] + [torch.empty((n >> r) * 4, dtype=torch.int64, device="cuda") for r in range(1, rounds)]
+        ptree_ptrs = [t.data_ptr() for t in ptrees]
+        positions = np.random.default_rng(7).integers(0, n, 64, dtype=np.uint64)
+        prove = lambda: z.fri_commit_phase(F, log_n, 10, players, ptree_ptrs, lambda r, root: alpha,  # noqa: E731
+                                           stream=sptr)
+        # The openings through the C ABI into preallocated host buffers (the Python wrapper's
+        # unpacking into per-query lists is not library time).
+        import ctypes
+        nb = 32 if F.limbs == 4 else 8
+        per_query = sum(log_n - r - 1 for r in range(rounds))
+        q_vals = ctypes.create_string_buffer(64 * rounds * 2 * nb)
+        q_paths = ctypes.create_string_buffer(64 * per_query * 32)
+        q_layers = (ctypes.c_void_p * rounds)(*players[:rounds])
+        q_trees = (ctypes.c_void_p * rounds)(*ptree_ptrs)
+        q_pos = positions.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+        def queries():
+            z._check(z.lib().zntt_fri_query_extract(F.id, log_n, rounds, q_layers, q_trees, q_pos, 64, q_vals,
+                                                    q_paths, sptr))
         for _ in range(warmup):
             one()
             chain()
@@ -692,6 +715,14 @@ def run_fri_config(z, torch, stream, steps, warmup, log_n=24):
         ms_one = time_region(torch, stream, one, steps) / steps
         ms_chain = time_region(torch, stream, chain, steps) / steps
         ms_commit = time_region(torch, stream, commit, steps) / steps
+        layer_copy = layer.clone()  # the commit phase folds into bufs; layer 0 is only read
+        for _ in range(2):
+            prove()
+            queries()
+        ms_prove = time_region(torch, stream, prove, max(steps // 4, 2)) / max(steps // 4, 2)
+        ms_queries = time_region(torch, stream, queries, steps) / steps
+        assert torch.equal(layer, layer_copy)
+        del layer_copy, ptrees
         moved = (n + n // 2 + n // 2) * ew  # layer read, table read, half layer written
         out["fields"][F.name] = {
             "fold_ms": ms_one, "fold_value": (n // 2) / (ms_one * 1e-3), "unit": "output elements/s",
@@ -704,6 +735,10 @@ def run_fri_config(z, torch, stream, steps, warmup, log_n=24):
                                 "peak_source": "zntt_probe_blake3: chained compressions in registers"},
             "commit_note": "hashPair leaves + BLAKE3 Merkle tree, n - 1 single-block compressions; "
                            "the call copies the root to the host, inside the timed region",
+            "prove_commit_ms": ms_prove, "prove_queries_ms": ms_queries,
+            "prove_note": f"zntt_fri_commit_phase: {rounds} rounds of commit, root to the host, challenge "
+                          f"callback, fold (2^{log_n} -> 2^10); zntt_fri_query_extract: 64 openings "
+                          f"(pairs and Merkle paths of every round) to the host",
         }
         del layer, bufs, nodes
     return out

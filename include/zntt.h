@@ -255,6 +255,40 @@ int zntt_fri_fold_device(int field, const uint64_t* d_layer, uint32_t log_n, con
 int zntt_fri_commit_layer(int field, const uint64_t* d_layer, uint32_t log_n, uint8_t* d_nodes,
                           uint8_t* root_out, void* stream);
 
+/* The Fiat-Shamir challenge of FRI round `round`, computed by the caller's transcript
+ * (proveOn's absorbBytes(root) then challengeFieldChecked, root.zig:386-388): writes alpha
+ * in the field's scalar layout (Montgomery limbs below p; a small field's canonical value
+ * in word 0, the other words zero) and returns 0, or nonzero to stop the phase. */
+typedef int (*zntt_fri_challenge_fn)(void* user, uint32_t round, const uint8_t root[32], uint64_t alpha_out[4]);
+
+/* The commit phase of proveOn (libs/fri/src/root.zig:372-403) on resident layers:
+ * for r < rounds = log_domain - log_final, commit layer r (2^(log_domain - r)
+ * evaluations in d_layers[r]) into d_nodes[r] as zntt_fri_commit_layer does, copy its
+ * root to roots_out + 32 r, ask `challenge` for alpha_r, and fold layer r into
+ * d_layers[r + 1] with one shared 1/(2x) table.  d_layers holds rounds + 1 device
+ * vectors (d_layers[0] the evaluations), d_nodes rounds node arrays of
+ * 2^(log_domain - r) x 32 bytes.  Checks Config.rounds' size rules (root.zig:188-195:
+ * log_final < log_domain, log_final <= 12) and log_domain <= the two-adicity
+ * (ZNTT_ERR_ORDER_TOO_LARGE); a callback error or an alpha that is not a field element is
+ * ZNTT_ERR_INVALID_ARGUMENT.  Returns after the last fold has finished.  All four fields. */
+int zntt_fri_commit_phase(int field, uint32_t log_domain, uint32_t log_final, uint64_t* const* d_layers,
+                          uint8_t* const* d_nodes, uint8_t* roots_out, zntt_fri_challenge_fn challenge, void* user,
+                          void* stream);
+
+/* The openings of buildQueries (libs/fri/src/root.zig:551-571) from the commit phase's
+ * resident layers and trees, for num_queries positions e0 < 2^log_domain (the caller's
+ * challengeU64() % 2^log_domain): per query q and round r < rounds, with
+ * j = e0 mod 2^(log_domain - r - 1),
+ *   values_out + (q rounds + r) 2 NB: toBytes(f_r[j]) || toBytes(f_r[j + half])
+ *     (serializePair; NB = 32, 8 or 4 bytes),
+ *   paths_out: the siblings of leaf j in tree r from the leaf level up
+ *     (MerkleTree.prove, libs/merkle/src/merkle_tree.zig:206-233), log_domain - r - 1
+ *     digests of 32 bytes, queries one after another and rounds in order within one.
+ * Host outputs; the call waits for them. */
+int zntt_fri_query_extract(int field, uint32_t log_domain, uint32_t rounds, const uint64_t* const* d_layers,
+                           const uint8_t* const* d_nodes, const uint64_t* positions, size_t num_queries,
+                           uint8_t* values_out, uint8_t* paths_out, void* stream);
+
 /* ---- serving: a continuously batching request server ---------------------------
  * Requests carry pinned host buffers.  A worker thread admits them in FIFO
  * order while their device buffers fit the HBM budget, turns whatever is

@@ -313,3 +313,55 @@ def fri_commit_layer(field: int, layer: np.ndarray, log_n: int, workers: int = 1
     st = load().zo_fri_commit_layer(field, _p(np.ascontiguousarray(layer)), log_n, nodes.ctypes.data, workers)
     assert st == OK, st
     return nodes
+
+
+def element_bytes(field: int) -> int:
+    """F.NUM_BYTES: ceil(bits / 8) of the modulus (32, 32, 8, 4)."""
+    return {BN254_FR: 32, BLS12_381_FR: 32, GOLDILOCKS: 8, BABYBEAR: 4}[field]
+
+
+def to_bytes(field: int, slots: np.ndarray) -> list:
+    """toBytes of each Montgomery slot: the canonical value, NUM_BYTES little-endian bytes."""
+    canon = from_mont(field, np.ascontiguousarray(slots))
+    nb = element_bytes(field)
+    return [row.tobytes()[:nb] for row in canon]
+
+
+def fri_commit_phase(field: int, evals: np.ndarray, log_domain: int, log_final: int, challenge,
+                     workers: int = 1):
+    """The commit loop of proveOn (libs/fri/src/root.zig:372-403): per round, commit the
+    layer (hashPair leaves, BLAKE3 Merkle tree), take alpha = challenge(round, root) (a
+    Montgomery slot), fold.  Returns (roots, layers 0..rounds, node arrays 0..rounds-1)."""
+    layers, trees, roots = [np.ascontiguousarray(evals)], [], []
+    for r in range(log_domain - log_final):
+        log_n = log_domain - r
+        nodes = fri_commit_layer(field, layers[r], log_n, workers=workers)
+        trees.append(nodes)
+        roots.append(nodes[1].tobytes())
+        alpha = np.asarray(challenge(r, roots[r]), dtype=np.uint64)
+        layers.append(fri_fold(field, layers[r], log_n, alpha, workers=workers))
+    return roots, layers, trees
+
+
+def fri_query_extract(field: int, layers: list, trees: list, log_domain: int, rounds: int, positions) -> tuple:
+    """The openings of buildQueries (libs/fri/src/root.zig:551-571): per query and round,
+    serializePair(f_r[j], f_r[j + half]) with j = e mod half, e carried from round to round
+    (e = j), and MerkleTree.prove(j)'s siblings (libs/merkle/src/merkle_tree.zig:206-233):
+    node pos ^ 1 for pos = half + j, half + j >> 1, ... while pos > 1."""
+    values, paths = [], []
+    for e0 in positions:
+        e, vq, pq = int(e0), [], []
+        for r in range(rounds):
+            half = 1 << (log_domain - r - 1)
+            j = e % half
+            pair = to_bytes(field, layers[r][[j, j + half]])
+            vq.append(pair[0] + pair[1])
+            sib, pos = [], half + j
+            while pos > 1:
+                sib.append(trees[r][pos + 1 if pos % 2 == 0 else pos - 1].tobytes())
+                pos >>= 1
+            pq.append(sib)
+            e = j
+        values.append(vq)
+        paths.append(pq)
+    return values, paths

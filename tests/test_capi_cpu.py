@@ -117,6 +117,27 @@ def test_poly_mul_contract_before_any_device_work(zntt, oracle):
         zntt._check(zntt.lib().zntt_poly_mul(0, None, 2, None, 0, 4, None, None))
 
 
+def test_fri_prover_loop_arguments_before_any_device_work(zntt):
+    """The commit phase and the query openings check Config.rounds' size rules
+    (libs/fri/src/root.zig:188-195), the field and their pointers before they look for a device."""
+    F = zntt.BN254_FR
+    never = lambda r, root: [0, 0, 0, 0]  # noqa: E731
+    for log_domain, log_final in ((4, 4), (4, 5), (0, 0), (20, 13)):
+        with pytest.raises(zntt.InvalidArgument):
+            zntt.fri_commit_phase(F, log_domain, log_final, [1] * 30, [1] * 30, never)
+    with pytest.raises(zntt.InvalidArgument):
+        zntt.fri_commit_phase(F, 6, 2, [1, 1, 0, 1, 1], [1] * 4, never)  # a null layer
+    with pytest.raises(zntt.UnsupportedField):
+        zntt.fri_commit_phase(zntt.Field(9, "bogus", 7, 1), 6, 2, [1] * 5, [1] * 4, never)
+    for log_domain, rounds in ((6, 0), (6, 7), (32, 4)):
+        with pytest.raises(zntt.InvalidArgument):
+            zntt.fri_query_extract(F, log_domain, rounds, [1] * 8, [16] * 8, [0])
+    with pytest.raises(zntt.InvalidArgument):
+        zntt.fri_query_extract(F, 6, 2, [1] * 3, [16] * 3, [64])  # a position outside the domain
+    with pytest.raises(zntt.InvalidArgument):
+        zntt.fri_query_extract(F, 6, 2, [1] * 3, [16] * 3, [])  # no queries
+
+
 def test_small_fields_host_side(zntt, oracle):
     """Goldilocks and BabyBear: field info, primitive roots as zig-field derives them (the
     roots of the reference's KAT, libs/ntt/src/root.zig:437-447, and the oracle's at every

@@ -1,7 +1,9 @@
-"""FRI's data-parallel prover steps on the device (zntt_fri_domain_fill, zntt_fri_fold_device)
-against the oracle's restatement of Domain.fill and the proveOn fold round
-(libs/fri/src/root.zig:133-166, 396-403) on all four fields, fold chains sharing one table, and
-at full size the fold identity fold(evals of p) = evals of p_even + alpha p_odd.  Needs a B200."""
+"""FRI's data-parallel prover steps on the device (zntt_fri_domain_fill, zntt_fri_fold_device,
+zntt_fri_commit_layer, zntt_fri_commit_phase, zntt_fri_query_extract) against the oracle's
+restatement of Domain.fill, the proveOn fold round and commit loop, and buildQueries
+(libs/fri/src/root.zig:133-166, 372-403, 551-571) on all four fields; fold chains sharing one
+table; at full size the fold identity fold(evals of p) = evals of p_even + alpha p_odd; and
+every opened path authenticates against its round's root.  Needs a B200."""
 from __future__ import annotations
 
 import os
@@ -196,3 +198,95 @@ def test_blake3_probe(z):
     """The commitment's roofline probe runs and gives a plausible compression rate."""
     rate = z.probe_blake3()
     assert 1e9 < rate < 1e13
+
+
+def _transcript(fid):
+    """A stand-in for the caller's transcript: alpha_r = 1 + the root's first three bytes
+    (little-endian) + 2^24 r, a field element of every field, as an oracle slot."""
+    def alpha(r, root):
+        return O.to_mont(fid, O.from_ints([1 + int.from_bytes(root[:3], "little") + (r << 24)]))[0]
+    return alpha
+
+
+def _prover_buffers(F, log_domain, log_final):
+    torch = _torch()
+    rounds = log_domain - log_final
+    layers = [torch.empty((1 << (log_domain - r)) * F.limbs, dtype=torch.int64, device="cuda")
+              for r in range(rounds + 1)]
+    trees = [torch.empty((1 << (log_domain - r)) * 4, dtype=torch.int64, device="cuda") for r in range(rounds)]
+    return layers, trees
+
+
+def _verify_path(root, index, leaf_bytes, siblings):
+    """MerkleTree.verify (libs/merkle/src/merkle_tree.zig:236-260) over BLAKE3: the side of each
+    sibling comes from the index."""
+    cur = O.blake3(leaf_bytes)
+    for sib in siblings:
+        cur = O.blake3(cur + sib if index % 2 == 0 else sib + cur)
+        index >>= 1
+    return cur == root
+
+
+def _check_prover(z, F, fid, log_domain, log_final, seed, num_queries):
+    torch = _torch()
+    rounds = log_domain - log_final
+    evals = O.random_elements(fid, seed, 1 << log_domain)
+    layers, trees = _prover_buffers(F, log_domain, log_final)
+    layers[0].copy_(_to_dev(F, evals))
+    torch.cuda.synchronize()
+    transcript = _transcript(fid)
+    roots = z.fri_commit_phase(F, log_domain, log_final, [t.data_ptr() for t in layers],
+                               [t.data_ptr() for t in trees], lambda r, root: _scalar(F, transcript(r, root)))
+    want_roots, want_layers, want_trees = O.fri_commit_phase(fid, evals, log_domain, log_final, transcript,
+                                                             workers=WORKERS)
+    assert roots == want_roots, F.name
+    for r in range(rounds + 1):
+        np.testing.assert_array_equal(_from_dev(F, layers[r]), want_layers[r], err_msg=f"{F.name} layer {r}")
+    for r in range(rounds):
+        np.testing.assert_array_equal(trees[r].cpu().numpy().view(np.uint8).reshape(-1, 32)[1:],
+                                      want_trees[r][1:], err_msg=f"{F.name} tree {r}")
+    positions = np.random.default_rng(seed).integers(0, 1 << log_domain, num_queries, dtype=np.uint64)
+    values, paths = z.fri_query_extract(F, log_domain, rounds, [t.data_ptr() for t in layers[:rounds]],
+                                        [t.data_ptr() for t in trees], positions)
+    want_values, want_paths = O.fri_query_extract(fid, want_layers, want_trees, log_domain, rounds, positions)
+    assert values == want_values and paths == want_paths, F.name
+    for q, e0 in enumerate(positions):
+        for r in range(rounds):
+            j = int(e0) % (1 << (log_domain - r - 1))
+            assert _verify_path(roots[r], j, values[q][r], paths[q][r]), (F.name, q, r)
+
+
+def test_commit_phase_and_queries_match_oracle(z):
+    """proveOn's commit loop (root.zig:372-403) and buildQueries' openings (root.zig:551-571) on
+    the device equal the oracle's, layer by layer and tree by tree, down to a final layer of 2^0
+    and 2^3 evaluations; every opened path authenticates against its round's root."""
+    for F, fid in _all(z):
+        _check_prover(z, F, fid, 11, 3, 500 + F.id, 16)
+        _check_prover(z, F, fid, 6, 0, 520 + F.id, 5)
+
+
+def test_commit_phase_full_size(z):
+    """2^20 BN254-Fr and 2^22 Goldilocks evaluations folded to 2^8 / 2^10 with 32 queries."""
+    everything = _all(z)
+    for (F, fid), log_domain, log_final in ((everything[0], 20, 8), (everything[2], 22, 10)):
+        _check_prover(z, F, fid, log_domain, log_final, 540 + F.id, 32)
+
+
+def test_commit_phase_errors(z):
+    """A callback error stops the phase with the caller's exception; an alpha outside the field
+    is InvalidArgument; a domain beyond the two-adicity is OrderTooLarge (proveOn's check,
+    root.zig:347)."""
+    F, fid = _all(z)[0]
+    layers, trees = _prover_buffers(F, 8, 4)
+    lp, tp = [t.data_ptr() for t in layers], [t.data_ptr() for t in trees]
+
+    def boom(r, root):
+        raise KeyError("transcript failed")
+    with pytest.raises(KeyError):
+        z.fri_commit_phase(F, 8, 4, lp, tp, boom)
+    with pytest.raises(z.InvalidArgument):
+        z.fri_commit_phase(F, 8, 4, lp, tp, lambda r, root: [2**64 - 1] * 4)
+    with pytest.raises(z.InvalidArgument):
+        z.fri_commit_phase(z.GOLDILOCKS, 8, 4, lp, tp, lambda r, root: [z.GOLDILOCKS.modulus, 0, 0, 0])
+    with pytest.raises(z.OrderTooLarge):
+        z.fri_commit_phase(z.BABYBEAR, 28, 12, [1] * 17, [16] * 16, lambda r, root: [1, 0, 0, 0])

@@ -162,6 +162,11 @@ class ServerStats(ctypes.Structure):
                                                "max_batch_ns")]
 
 
+# zntt_fri_challenge_fn: (user, round, root[32], alpha_out[4]) -> status.
+FRI_CHALLENGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint32,
+                                    ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint64))
+
+
 class Job(ctypes.Structure):
     """zntt_job (include/zntt.h)."""
     _fields_ = [("kind", ctypes.c_int), ("mode", ctypes.c_int), ("tw", ctypes.c_void_p),
@@ -213,6 +218,10 @@ def lib():
         L.zntt_poly_mul_device.argtypes = [vp, vp, sz, vp, sz, vp, vp]
         L.zntt_fri_domain_fill.argtypes = [i, ctypes.c_uint32, vp, vp]
         L.zntt_fri_fold_device.argtypes = [i, vp, ctypes.c_uint32, _U64P, vp, ctypes.c_uint32, vp]
+        L.zntt_fri_commit_phase.argtypes = [i, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(vp),
+                                            ctypes.POINTER(vp), ctypes.c_char_p, FRI_CHALLENGE_FN, vp, vp]
+        L.zntt_fri_query_extract.argtypes = [i, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(vp),
+                                             ctypes.POINTER(vp), _U64P, sz, ctypes.c_char_p, ctypes.c_char_p, vp]
         L.zntt_fri_commit_layer.argtypes = [i, vp, ctypes.c_uint32, vp, ctypes.c_char_p, vp]
         L.zntt_poly_mul.argtypes = [i, _U64P, sz, _U64P, sz, sz, _U64P, ctypes.POINTER(ctypes.c_int64)]
         L.zntt_autotune.argtypes = [i, ctypes.c_uint32, ctypes.c_uint32]
@@ -583,6 +592,66 @@ def fri_fold(F: Field, d_layer: int, log_n: int, alpha, d_out: int, log_table: i
     into 2^(log_n - 1); `alpha` in the field's scalar form (4 Montgomery limbs, or [value, 0, 0, 0])."""
     _ensure_init()
     _check(lib().zntt_fri_fold_device(F.id, d_layer, log_n, _root(alpha), d_out, log_table, stream or None))
+
+
+def fri_commit_phase(F: Field, log_domain: int, log_final: int, d_layers, d_nodes, challenge,
+                     stream: int = 0) -> list:
+    """The commit phase of proveOn (libs/fri/src/root.zig:372-403) on device layers: d_layers
+    holds rounds + 1 device pointers (d_layers[0] the evaluations), d_nodes rounds node arrays;
+    challenge(round, root: bytes) returns alpha in the field's scalar form (4 Montgomery limbs,
+    or [value, 0, 0, 0]).  Returns the rounds' roots.  An exception in the callback stops the
+    phase and is raised again here."""
+    _ensure_init()
+    rounds = log_domain - log_final
+    raised = []
+
+    def cb(_user, rnd, root, alpha_out):
+        try:
+            a = _root(challenge(int(rnd), bytes(root[:32])))
+            for k in range(4):
+                alpha_out[k] = int(a[k])
+            return 0
+        except BaseException as e:  # noqa: BLE001 -- reported after the C call returns
+            raised.append(e)
+            return 1
+
+    fn = FRI_CHALLENGE_FN(cb)
+    layers = (ctypes.c_void_p * len(d_layers))(*d_layers)
+    nodes = (ctypes.c_void_p * max(len(d_nodes), 1))(*d_nodes)
+    roots = ctypes.create_string_buffer(32 * max(rounds, 1))
+    status = lib().zntt_fri_commit_phase(F.id, log_domain, log_final, layers, nodes, roots, fn, None, stream or None)
+    if raised:
+        raise raised[0]
+    _check(status)
+    return [roots.raw[32 * r:32 * (r + 1)] for r in range(rounds)]
+
+
+def fri_query_extract(F: Field, log_domain: int, rounds: int, d_layers, d_nodes, positions, stream: int = 0):
+    """The openings of buildQueries (libs/fri/src/root.zig:551-571) from resident layers and
+    trees: returns (values, paths) with values[q][r] = serializePair bytes of round r's pair and
+    paths[q][r] = the list of sibling digests of MerkleTree.prove, leaf level first."""
+    _ensure_init()
+    nb = 32 if F.limbs == 4 else (8 if F.id == GOLDILOCKS.id else 4)
+    pos = np.ascontiguousarray(np.asarray(positions, dtype=np.uint64))
+    nq = len(pos)
+    per_query = sum(log_domain - r - 1 for r in range(rounds))
+    vals = ctypes.create_string_buffer(max(nq * rounds * 2 * nb, 1))
+    paths = ctypes.create_string_buffer(max(nq * per_query * 32, 1))
+    layers = (ctypes.c_void_p * max(len(d_layers), 1))(*d_layers)
+    nodes = (ctypes.c_void_p * max(len(d_nodes), 1))(*d_nodes)
+    _check(lib().zntt_fri_query_extract(F.id, log_domain, rounds, layers, nodes,
+                                        pos.ctypes.data_as(_U64P) if nq else None, nq, vals, paths, stream or None))
+    vraw, praw = vals.raw, paths.raw  # one copy each (.raw copies the whole buffer)
+    values, out_paths, off = [], [], 0
+    for q in range(nq):
+        values.append([vraw[(q * rounds + r) * 2 * nb:(q * rounds + r + 1) * 2 * nb] for r in range(rounds)])
+        per_round = []
+        for r in range(rounds):
+            depth = log_domain - r - 1
+            per_round.append([praw[(off + k) * 32:(off + k + 1) * 32] for k in range(depth)])
+            off += depth
+        out_paths.append(per_round)
+    return values, out_paths
 
 
 def fri_commit_layer(F: Field, d_layer: int, log_n: int, d_nodes: int, stream: int = 0) -> bytes:
