@@ -365,3 +365,33 @@ def fri_query_extract(field: int, layers: list, trees: list, log_domain: int, ro
         values.append(vq)
         paths.append(pq)
     return values, paths
+
+
+def fri_prove(field: int, evals: np.ndarray, log_domain: int, log_final: int, log_residual: int, num_queries: int,
+              transcript, workers: int = 1) -> dict:
+    """proveOn over Domain(F) (libs/fri/src/root.zig:335-503) on the oracle's commitment, fold
+    and inverse transform: the commit loop above with alpha = transcript.absorb_bytes(root),
+    challenge_field_checked (root.zig:386-388); the residual = the first 2^log_residual
+    coefficients of the final layer's interpolant (interpolateToCoeffs, the unique polynomial
+    of degree < 2^log_final: its inverse transform), absorbed as toBytes; then num_queries
+    positions challengeU64() % 2^log_domain and their openings.  `transcript` is the caller's
+    (absorb_bytes, challenge_field_checked(p, num_bytes), challenge_u64)."""
+    p, nb = MODULI[field], element_bytes(field)
+
+    def challenge(_r, root):
+        transcript.absorb_bytes(root)
+        return to_mont(field, from_ints([transcript.challenge_field_checked(p, nb)]))[0]
+
+    rounds = log_domain - log_final
+    roots, layers, trees = fri_commit_phase(field, evals, log_domain, log_final, challenge, workers=workers)
+    coeffs = np.ascontiguousarray(layers[rounds].copy())
+    st, g = primitive_root(field, log_final)
+    assert st == OK and intt(field, coeffs, log_final, g) == OK
+    residual = to_bytes(field, coeffs[:1 << log_residual])
+    for cb in residual:
+        transcript.absorb_bytes(cb)
+    positions = [transcript.challenge_u64() % (1 << log_domain) for _ in range(num_queries)]
+    values, paths = fri_query_extract(field, layers, trees, log_domain, rounds, positions)
+    return {"roots": roots, "residual": residual,
+            "queries": [{"pair_index": e0, "values": values[q], "paths": paths[q]} for q, e0 in enumerate(positions)],
+            "log_domain": log_domain, "log_final": log_final, "log_residual_degree": log_residual}

@@ -24,6 +24,11 @@ Two kinds of fixture:
      fields: seeded factors of several lengths, trailing zero coefficients
      (normalized away), a zero factor, constants, and max_degree cases that
      fit exactly or raise DegreeTooLarge.
+   * fri_proof.json -- the reference's transcript known answer (four Goldilocks
+     challenges from Transcript.init("wire-compat"), libs/fri/src/root.zig, copied as
+     data and reproduced by pyref.Transcript) and whole FRI proofs of pyref.fri_prove
+     over that transcript for low-degree evaluations in all four fields, each accepted
+     by pyref.fri_verify.
 
 Values are canonical (not Montgomery) hex strings.  Large vectors are stored as
 a SHA-256 of their little-endian 32-byte encoding plus a few leading values.
@@ -196,6 +201,50 @@ def fri_commit_cases(ref: str) -> dict:
     return {"kat": kat, "empty": pyref.blake3(b"").hex(), "cases": cases}
 
 
+def parse_transcript_kat(ref: str) -> dict:
+    """The reference's challenge-sequence known answer (libs/fri/src/root.zig, test "fri: the
+    transcript switch preserved the challenge sequence"): four Goldilocks challenges from
+    Transcript.init("wire-compat"), toBytes concatenated."""
+    path = os.path.join(ref, "libs/fri/src/root.zig")
+    text = open(path).read()
+    start = text.index('test "fri: the transcript switch preserved the challenge sequence"')
+    m = re.search(r'if \(F == Goldilocks\)\s*"([0-9a-f]+)"', text[start:])
+    label = re.search(r'Transcript\.init\("([^"]+)"\)', text[start:]).group(1)
+    lineno = text[:start + m.start(1)].count("\n") + 1
+    return {"label": label, "field": "goldilocks", "draws": 4, "expect": m.group(1),
+            "source": f"libs/fri/src/root.zig:{lineno}"}
+
+
+FRI_FIELDS = [("bn254_fr", pyref.BN254_FR_P, 32), ("bls12_381_fr", pyref.BLS12_381_FR_P, 32),
+              ("goldilocks", 0xFFFFFFFF00000001, 8), ("babybear", 0x78000001, 4)]
+
+
+def fri_proof_cases(ref: str) -> dict:
+    """Whole FRI proofs of the pure-Python prove (pyref.fri_prove) over the reference's
+    transcript, for the evaluations of a polynomial of degree < 2^log_initial_degree on the
+    2^log_domain subgroup; each verifies under pyref.fri_verify."""
+    kat = parse_transcript_kat(ref)
+    t = pyref.Transcript(kat["label"].encode())
+    got = b"".join(t.challenge_field_checked(0xFFFFFFFF00000001, 8).to_bytes(8, "little") for _ in range(4))
+    assert got.hex() == kat["expect"], "transcript restatement differs from the reference's known answer"
+    cfg = {"log_domain": 8, "log_initial_degree": 6, "log_final": 3, "log_residual_degree": 1, "num_queries": 3,
+           "label": "zig-algebra-b200 fri golden"}
+    cases = []
+    for q, (name, p, nb) in enumerate(FRI_FIELDS):
+        n = 1 << cfg["log_domain"]
+        coeffs = pyref.random_field_values(p, 1100 + q, 1 << cfg["log_initial_degree"])
+        evals = pyref.fft(coeffs + [0] * (n - len(coeffs)), pyref.primitive_root(p, cfg["log_domain"]), p)
+        args = (cfg["log_domain"], cfg["log_final"], cfg["log_residual_degree"], cfg["num_queries"])
+        proof = pyref.fri_prove(p, nb, pyref.Transcript(cfg["label"].encode()), evals, *args)
+        assert pyref.fri_verify(p, nb, pyref.Transcript(cfg["label"].encode()), proof, *args)
+        cases.append({"field": name, "evals": [hex(v) for v in evals],
+                      "roots": [r.hex() for r in proof["roots"]], "residual": [c.hex() for c in proof["residual"]],
+                      "queries": [{"pair_index": qq["pair_index"], "values": [v.hex() for v in qq["values"]],
+                                   "paths": [[x.hex() for x in path] for path in qq["paths"]]}
+                                  for qq in proof["queries"]]})
+    return {"transcript_kat": kat, "config": cfg, "cases": cases}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -206,6 +255,7 @@ def main() -> None:
     json.dump(lde_case(), open(os.path.join(HERE, "coset_lde.json"), "w"), indent=1)
     json.dump(poly_cases(), open(os.path.join(HERE, "poly_mul.json"), "w"), indent=1)
     json.dump(fri_commit_cases(args.reference), open(os.path.join(HERE, "fri_commit.json"), "w"), indent=1)
+    json.dump(fri_proof_cases(args.reference), open(os.path.join(HERE, "fri_proof.json"), "w"), indent=1)
     print("fixtures written to", HERE)
 
 

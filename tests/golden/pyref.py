@@ -19,6 +19,10 @@ the three is evidence rather than self-consistency:
 * Roots of unity as the reference derives them (libs/field/src/roots.zig:149-158):
   z = the first quadratic non-residue counting up from 2, raised to
   odd_part << (two_adicity - log_n).
+* The Fiat-Shamir transcript of libs/transcript/src/root.zig:38-170 (length-
+  prefixed absorbs into one BLAKE3 message, squeeze = the digest, re-keyed with
+  it) and zig-fri's prove / verify (libs/fri/src/root.zig:335-503, 606-720) over
+  it, in field integers, for proofs whose transcript messages fit one chunk.
 """
 from __future__ import annotations
 
@@ -241,3 +245,158 @@ def fri_commit_layer(values: list[int], num_bytes: int) -> list[bytes]:
     for i in range(h - 1, 0, -1):
         nodes[i] = blake3(nodes[2 * i] + nodes[2 * i + 1])
     return nodes
+
+
+class Transcript:
+    """zig-transcript's Transcript (libs/transcript/src/root.zig:38-170).  The hasher state is
+    the message absorbed since the last re-key; a squeeze hashes it."""
+
+    def __init__(self, label: bytes):
+        self.msg = len(label).to_bytes(8, "little") + label
+
+    def absorb_bytes(self, data: bytes) -> None:
+        self.msg += len(data).to_bytes(8, "little") + data
+
+    def absorb_u64(self, v: int) -> None:
+        self.absorb_bytes(v.to_bytes(8, "little"))
+
+    def challenge_bytes(self, n: int) -> bytes:
+        digest = blake3(self.msg)
+        out = b""
+        while len(out) < n:
+            out += digest[:min(32, n - len(out))]
+            if len(out) < n:
+                digest = blake3(digest)
+        self.msg = digest  # re-key with the (last) digest
+        return out
+
+    def challenge_u64(self) -> int:
+        return int.from_bytes(self.challenge_bytes(8), "little")
+
+    def challenge_field_checked(self, p: int, num_bytes: int) -> int:
+        """challengeFieldChecked: NUM_BYTES little-endian bytes, rejected (and re-drawn) when >= p."""
+        while True:
+            v = int.from_bytes(self.challenge_bytes(num_bytes), "little")
+            if v < p:
+                return v
+
+
+def fri_fold_values(f: list[int], alpha: int, p: int) -> list[int]:
+    """One fold round (libs/fri/src/root.zig:396-403) on the natural-order subgroup of order len(f)."""
+    n = len(f)
+    h = n // 2
+    g = primitive_root(p, n.bit_length() - 1)
+    inv2 = pow(2, -1, p)
+    out = []
+    for j in range(h):
+        x = pow(g, j, p)
+        even = (f[j] + f[j + h]) * inv2 % p
+        odd = (f[j] - f[j + h]) * pow(x, -1, p) * inv2 % p
+        out.append((even + alpha * odd) % p)
+    return out
+
+
+def merkle_siblings(nodes: list[bytes], leaf_count: int, index: int) -> list[bytes]:
+    """MerkleTree.prove's siblings (libs/merkle/src/merkle_tree.zig:206-233), leaf level first."""
+    out, pos = [], leaf_count + index
+    while pos > 1:
+        out.append(nodes[pos ^ 1])
+        pos >>= 1
+    return out
+
+
+def fri_prove(p: int, num_bytes: int, transcript: Transcript, evals: list[int], log_domain: int, log_final: int,
+              log_residual: int, num_queries: int) -> dict:
+    """proveOn (libs/fri/src/root.zig:335-503) over Domain(F): commit, absorb the root, draw
+    alpha, fold, per round; the residual = the first 2^log_residual coefficients of the final
+    layer's interpolant (interpolateToCoeffs), absorbed; then per query e0 = challengeU64 % n
+    and, per round, the pair at j = e mod half and its Merkle path (buildQueries)."""
+    rounds = log_domain - log_final
+    layers, trees, roots = [list(evals)], [], []
+    for r in range(rounds):
+        nodes = fri_commit_layer(layers[r], num_bytes)
+        trees.append(nodes)
+        roots.append(nodes[1])
+        transcript.absorb_bytes(nodes[1])
+        alpha = transcript.challenge_field_checked(p, num_bytes)
+        layers.append(fri_fold_values(layers[r], alpha, p))
+    coeffs = inverse_transform(layers[rounds], primitive_root(p, log_final), p)
+    residual = [to_bytes(c, num_bytes) for c in coeffs[:1 << log_residual]]
+    for cb in residual:
+        transcript.absorb_bytes(cb)
+    queries = []
+    for _ in range(num_queries):
+        e0 = transcript.challenge_u64() % (1 << log_domain)
+        e, values, paths = e0, [], []
+        for r in range(rounds):
+            half = len(layers[r]) // 2
+            j = e % half
+            values.append(to_bytes(layers[r][j], num_bytes) + to_bytes(layers[r][j + half], num_bytes))
+            paths.append(merkle_siblings(trees[r], half, j))
+            e = j
+        queries.append({"pair_index": e0, "values": values, "paths": paths})
+    return {"roots": roots, "residual": residual, "queries": queries, "log_domain": log_domain,
+            "log_final": log_final, "log_residual_degree": log_residual}
+
+
+def fri_verify(p: int, num_bytes: int, transcript: Transcript, proof: dict, log_domain: int, log_final: int,
+               log_residual: int, num_queries: int) -> bool:
+    """verifyOn (libs/fri/src/root.zig:606-720) over Domain(F): replay the challenges, evaluate
+    the residual on the final domain, and per query check the pair index, every Merkle path
+    (MerkleTree.verifyPath: the sibling's side from the index), the fold into the next round's
+    pair and, in the last round, into the residual's evaluation."""
+    rounds = log_domain - log_final
+    if (proof["log_domain"], proof["log_final"], proof["log_residual_degree"]) != (log_domain, log_final,
+                                                                                 log_residual):
+        return False
+    if len(proof["roots"]) != rounds or len(proof["residual"]) != 1 << log_residual:
+        return False
+    if len(proof["queries"]) != num_queries:
+        return False
+    alphas = []
+    for root in proof["roots"]:
+        transcript.absorb_bytes(root)
+        alphas.append(transcript.challenge_field_checked(p, num_bytes))
+    residual = []
+    for cb in proof["residual"]:
+        c = int.from_bytes(cb, "little")
+        if len(cb) != num_bytes or c >= p:
+            return False
+        residual.append(c)
+        transcript.absorb_bytes(cb)
+    gf = primitive_root(p, log_final)
+    final = [sum(c * pow(gf, i * k, p) for k, c in enumerate(residual)) % p for i in range(1 << log_final)]
+    inv2 = pow(2, -1, p)
+    for q in proof["queries"]:
+        if q["pair_index"] != transcript.challenge_u64() % (1 << log_domain):
+            return False
+        if len(q["values"]) != rounds or len(q["paths"]) != rounds:
+            return False
+        e = q["pair_index"]
+        for r in range(rounds):
+            layer_log = log_domain - r
+            half = (1 << layer_log) // 2
+            j = e % half
+            vb = q["values"][r]
+            x, negx = int.from_bytes(vb[:num_bytes], "little"), int.from_bytes(vb[num_bytes:], "little")
+            if len(vb) != 2 * num_bytes or x >= p or negx >= p:
+                return False
+            cur, idx = blake3(vb), j
+            if len(q["paths"][r]) != layer_log - 1:
+                return False
+            for sib in q["paths"][r]:
+                cur = blake3(cur + sib if idx % 2 == 0 else sib + cur)
+                idx >>= 1
+            if cur != proof["roots"][r]:
+                return False
+            xv = pow(primitive_root(p, layer_log), j, p)
+            expected = ((x + negx) * inv2 + alphas[r] * (x - negx) * pow(xv, -1, p) * inv2) % p
+            if r + 1 < rounds:
+                nb = q["values"][r + 1]
+                slot = 0 if j < half // 2 else 1
+                if expected != int.from_bytes(nb[slot * num_bytes:(slot + 1) * num_bytes], "little"):
+                    return False
+            elif expected != final[j]:
+                return False
+            e = j
+    return True

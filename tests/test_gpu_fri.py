@@ -290,3 +290,76 @@ def test_commit_phase_errors(z):
         z.fri_commit_phase(z.GOLDILOCKS, 8, 4, lp, tp, lambda r, root: [z.GOLDILOCKS.modulus, 0, 0, 0])
     with pytest.raises(z.OrderTooLarge):
         z.fri_commit_phase(z.BABYBEAR, 28, 12, [1] * 17, [16] * 16, lambda r, root: [1, 0, 0, 0])
+
+
+def _proof_dict(proof):
+    return {"roots": proof.roots, "residual": proof.residual, "queries": proof.queries,
+            "log_domain": proof.log_domain, "log_final": proof.log_final,
+            "log_residual_degree": proof.log_residual_degree}
+
+
+def test_device_prove_matches_fixture(z):
+    """zig-fri's prove on the device (fri_prove: commit phase, residual, openings) over the
+    reference's transcript equals the pure-Python proofs of fri_proof.json byte for byte, on
+    all four fields."""
+    import json
+    import pyref
+    d = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fri_proof.json")))
+    cfg = d["config"]
+    config = z.FriConfig(cfg["log_domain"], cfg["log_initial_degree"], cfg["log_final"], cfg["log_residual_degree"],
+                         cfg["num_queries"])
+    names = {F.name: (F, fid) for F, fid in _all(z)}
+    for c in d["cases"]:
+        F, fid = names[c["field"]]
+        dev = _to_dev(F, O.to_mont(fid, O.from_ints([int(v, 16) for v in c["evals"]])))
+        proof = z.fri_prove(F, pyref.Transcript(cfg["label"].encode()), dev.data_ptr(), config)
+        assert [r.hex() for r in proof.roots] == c["roots"], F.name
+        assert [x.hex() for x in proof.residual] == c["residual"], F.name
+        got_q = [{"pair_index": int(q["pair_index"]), "values": [v.hex() for v in q["values"]],
+                  "paths": [[x.hex() for x in path] for path in q["paths"]]} for q in proof.queries]
+        assert got_q == c["queries"], F.name
+
+
+def test_device_prove_full_size_verifies(z):
+    """Honest proofs of low-degree evaluations made on the device (the evaluations themselves a
+    device transform of 2^16 coefficients): 2^20 BN254-Fr and 2^22 Goldilocks, final layers of
+    2^8 and 2^10, a residual of 2^4 coefficients and 32 queries.  Each equals the oracle's
+    proof and passes the restated verifier; random (not low-degree) evaluations are rejected
+    (the reference's regression test, libs/fri/src/root.zig:775)."""
+    import pyref
+    torch = _torch()
+    everything = _all(z)
+    for (F, fid), log_domain, log_final in ((everything[0], 20, 8), (everything[2], 22, 10)):
+        rounds = log_domain - log_final
+        config = z.FriConfig(log_domain, rounds + 4, log_final, 4, 32)
+        n = 1 << log_domain
+        coeffs = np.zeros((n, 4), dtype=np.uint64)
+        coeffs[:1 << (rounds + 4)] = O.random_elements(fid, 600 + log_domain, 1 << (rounds + 4))
+        src = _to_dev(F, coeffs)
+        evals = torch.empty_like(src)
+        with z.DeviceTwiddles(F, log_domain, z.primitiveRootOfUnity(F, log_domain)) as tw:
+            z.ntt_device(tw, src.data_ptr(), evals.data_ptr(), z.FORWARD)
+        torch.cuda.synchronize()
+        label = b"fri full size"
+        proof = z.fri_prove(F, pyref.Transcript(label), evals.data_ptr(), config)
+        want = O.fri_prove(fid, _from_dev(F, evals), log_domain, log_final, 4, 32, pyref.Transcript(label),
+                           workers=WORKERS)
+        assert _proof_dict(proof) == want, F.name
+        p, nb = O.MODULI[fid], O.element_bytes(fid)
+        assert pyref.fri_verify(p, nb, pyref.Transcript(label), want, log_domain, log_final, 4, 32), F.name
+        noise = _to_dev(F, O.random_elements(fid, 700 + log_domain, n))
+        bad = z.fri_prove(F, pyref.Transcript(label), noise.data_ptr(), config)
+        assert not pyref.fri_verify(p, nb, pyref.Transcript(label), _proof_dict(bad), log_domain, log_final, 4, 32)
+        del src, evals, noise
+        torch.cuda.empty_cache()
+
+
+def test_prove_config_checks(z):
+    """Config.rounds / Config.validate (libs/fri/src/root.zig:188-202) and proveOn's
+    two-adicity check refuse bad parameters before any device work."""
+    import pyref
+    for args in ((10, 6, 4, 2, 0), (10, 6, 4, 4, 3), (10, 6, 13, 2, 3), (10, 5, 4, 2, 3), (10, 11, 4, 2, 3)):
+        with pytest.raises(z.InvalidArgument):
+            z.fri_prove(z.BN254_FR, pyref.Transcript(b"x"), 1, z.FriConfig(*args))
+    with pytest.raises(z.InvalidArgument):
+        z.fri_prove(z.BABYBEAR, pyref.Transcript(b"x"), 1, z.FriConfig(28, 20, 10, 2, 3))

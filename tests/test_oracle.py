@@ -325,3 +325,59 @@ def test_blake3_and_fri_commitment_fixture():
         assert nodes[1].tobytes().hex() == c["root"], (c["field"], c["log_n"])
         if "nodes" in c:
             assert [x.tobytes().hex() for x in nodes[1:]] == c["nodes"]
+
+
+def _proof_hex(proof):
+    return {"roots": [r.hex() for r in proof["roots"]], "residual": [c.hex() for c in proof["residual"]],
+            "queries": [{"pair_index": int(q["pair_index"]), "values": [v.hex() for v in q["values"]],
+                         "paths": [[x.hex() for x in path] for path in q["paths"]]} for q in proof["queries"]]}
+
+
+def _proof_bytes(c, cfg):
+    return {"roots": [bytes.fromhex(r) for r in c["roots"]], "residual": [bytes.fromhex(x) for x in c["residual"]],
+            "queries": [{"pair_index": q["pair_index"], "values": [bytes.fromhex(v) for v in q["values"]],
+                         "paths": [[bytes.fromhex(x) for x in path] for path in q["paths"]]} for q in c["queries"]],
+            "log_domain": cfg["log_domain"], "log_final": cfg["log_final"],
+            "log_residual_degree": cfg["log_residual_degree"]}
+
+
+def test_transcript_known_answer():
+    """pyref.Transcript (libs/transcript/src/root.zig:38-170) against the reference's own
+    challenge-sequence known answer (libs/fri/src/root.zig, "wire-compat", Goldilocks)."""
+    kat = json.load(open(os.path.join(GOLDEN, "fri_proof.json")))["transcript_kat"]
+    t = pyref.Transcript(kat["label"].encode())
+    got = b"".join(t.challenge_field_checked(0xFFFFFFFF00000001, 8).to_bytes(8, "little")
+                   for _ in range(kat["draws"]))
+    assert got.hex() == kat["expect"], kat["source"]
+
+
+def test_fri_proof_fixture_oracle_and_verifier():
+    """The oracle's prove (commitment, fold and inverse transform in C++) reproduces the
+    pure-Python proofs of fri_proof.json on all four fields; the restated verifier accepts
+    them and rejects a tampered value, a tampered path, a tampered residual and another
+    transcript label (the reference's own rejection tests, libs/fri/src/root.zig:834-902)."""
+    d = json.load(open(os.path.join(GOLDEN, "fri_proof.json")))
+    cfg = d["config"]
+    args = (cfg["log_domain"], cfg["log_final"], cfg["log_residual_degree"], cfg["num_queries"])
+    label = cfg["label"].encode()
+    for c in d["cases"]:
+        f = FIELD_IDS[c["field"]]
+        p, nb = O.MODULI[f], O.element_bytes(f)
+        evals = _mont_of(f, [int(v, 16) for v in c["evals"]])
+        got = O.fri_prove(f, evals, *args, pyref.Transcript(label), workers=4)
+        assert _proof_hex(got) == {k: c[k] for k in ("roots", "residual", "queries")}, c["field"]
+        proof = _proof_bytes(c, cfg)
+        assert pyref.fri_verify(p, nb, pyref.Transcript(label), proof, *args), c["field"]
+        assert not pyref.fri_verify(p, nb, pyref.Transcript(b"another statement"), proof, *args)
+        for where in ("value", "path", "residual"):
+            bad = json.loads(json.dumps(c))
+            if where == "value":
+                v = bad["queries"][1]["values"][2]
+                bad["queries"][1]["values"][2] = ("%02x" % (int(v[:2], 16) ^ 1)) + v[2:]
+            elif where == "path":
+                x = bad["queries"][0]["paths"][1][0]
+                bad["queries"][0]["paths"][1][0] = ("%02x" % (int(x[:2], 16) ^ 0x80)) + x[2:]
+            else:
+                x = bad["residual"][0]
+                bad["residual"][0] = ("%02x" % (int(x[:2], 16) ^ 1)) + x[2:]
+            assert not pyref.fri_verify(p, nb, pyref.Transcript(label), _proof_bytes(bad, cfg), *args), where

@@ -654,6 +654,90 @@ def fri_query_extract(F: Field, log_domain: int, rounds: int, d_layers, d_nodes,
     return values, out_paths
 
 
+class FriConfig:
+    """zig-fri's Config (libs/fri/src/root.zig:171-203)."""
+
+    def __init__(self, log_domain: int, log_initial_degree: int, log_final: int, log_residual_degree: int,
+                 num_queries: int):
+        self.log_domain, self.log_initial_degree = log_domain, log_initial_degree
+        self.log_final, self.log_residual_degree, self.num_queries = log_final, log_residual_degree, num_queries
+
+    def rounds(self) -> int:
+        """Config.rounds (root.zig:188-195); InvalidArgument for the reference's InvalidParameters."""
+        if self.log_domain == 0 or self.log_domain > 63 or self.log_final >= self.log_domain \
+                or self.log_residual_degree >= self.log_final or self.log_final > 12 \
+                or self.log_residual_degree > 12 or self.num_queries == 0:
+            raise InvalidArgument("invalid FRI parameters (Config.rounds)")
+        return self.log_domain - self.log_final
+
+    def validate(self) -> None:
+        """Config.validate (root.zig:197-202)."""
+        r = self.rounds()
+        if self.log_initial_degree > self.log_domain or self.log_initial_degree < r \
+                or self.log_initial_degree - r != self.log_residual_degree:
+            raise InvalidArgument("invalid FRI parameters (Config.validate)")
+
+
+class FriProof:
+    """zig-fri's Proof (libs/fri/src/root.zig:209-240): per round the Merkle root, the residual
+    coefficients' toBytes, and per query the pair index with each round's serializePair bytes
+    and Merkle siblings (leaf level first)."""
+
+    def __init__(self, roots, residual, queries, log_domain, log_final, log_residual_degree):
+        self.roots, self.residual, self.queries = roots, residual, queries
+        self.log_domain, self.log_final, self.log_residual_degree = log_domain, log_final, log_residual_degree
+
+
+def _num_bytes(F: Field) -> int:
+    return 32 if F.limbs == 4 else (8 if F.id == GOLDILOCKS.id else 4)
+
+
+def _canonical(F: Field, limbs) -> int:
+    v = sum(int(x) << (64 * k) for k, x in enumerate(limbs))
+    return v * pow(1 << 256, -1, F.modulus) % F.modulus if F.limbs == 4 else v
+
+
+def fri_prove(F: Field, transcript, d_evals: int, config: FriConfig, stream: int = 0) -> FriProof:
+    """zig-fri's prove (proveOn over Domain(F), libs/fri/src/root.zig:311-503) with the
+    evaluations resident on the device at d_evals (2^log_domain elements in F's layout, left
+    unchanged).  The transcript is the caller's, as in the reference: it needs
+    absorb_bytes(bytes), challenge_field_checked(modulus, num_bytes) -> int in [0, p) and
+    challenge_u64() -> int.  Layers, trees and folds stay on the device; the final layer's
+    interpolant comes from the library's inverse transform; only roots, the residual and the
+    openings cross to the host.  Device buffers are allocated with torch."""
+    import torch  # device allocation only
+    config.validate()
+    rounds = config.rounds()
+    if config.log_domain > F.two_adicity:
+        raise InvalidArgument("log_domain exceeds the field's two-adicity (proveOn)")
+    _ensure_init()
+    nb = _num_bytes(F)
+    n = 1 << config.log_domain
+    layers = [torch.empty((n >> r) * F.limbs, dtype=torch.int64, device="cuda") for r in range(1, rounds + 1)]
+    trees = [torch.empty((n >> r) * 4, dtype=torch.int64, device="cuda") for r in range(rounds)]
+    layer_ptrs = [d_evals] + [t.data_ptr() for t in layers]
+    tree_ptrs = [t.data_ptr() for t in trees]
+
+    def challenge(_r, root):
+        transcript.absorb_bytes(root)
+        a = transcript.challenge_field_checked(F.modulus, nb)
+        return to_montgomery(F, a) if F.limbs == 4 else np.array([a, 0, 0, 0], dtype=np.uint64)
+
+    roots = fri_commit_phase(F, config.log_domain, config.log_final, layer_ptrs, tree_ptrs, challenge, stream)
+    final = layers[-1].cpu().numpy().view(np.uint64)
+    final = final.reshape(-1, 4).copy() if F.limbs == 4 else final.copy()
+    intt(F, final, config.log_final, primitiveRootOfUnity(F, config.log_final))  # interpolateToCoeffs
+    residual = [_canonical(F, final[i] if F.limbs == 4 else [final[i]]).to_bytes(nb, "little")
+                for i in range(1 << config.log_residual_degree)]
+    for cb in residual:
+        transcript.absorb_bytes(cb)  # absorbField of the deserialized coefficient: the same bytes
+    positions = [transcript.challenge_u64() % n for _ in range(config.num_queries)]
+    values, paths = fri_query_extract(F, config.log_domain, rounds, layer_ptrs[:rounds], tree_ptrs, positions,
+                                      stream)
+    queries = [{"pair_index": e0, "values": values[q], "paths": paths[q]} for q, e0 in enumerate(positions)]
+    return FriProof(roots, residual, queries, config.log_domain, config.log_final, config.log_residual_degree)
+
+
 def fri_commit_layer(F: Field, d_layer: int, log_n: int, d_nodes: int, stream: int = 0) -> bytes:
     """The FRI layer commitment (hashPair leaves, heap-ordered BLAKE3 Merkle tree) of a device
     layer of 2^log_n evaluations into d_nodes (2^log_n x 32 bytes); returns the root."""
