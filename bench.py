@@ -333,6 +333,7 @@ def run_zntt(args, rank, world, local):
     z.ntt_host_many(tw, ptrs, z.FORWARD)
     e2e_s = max_over_ranks(time.perf_counter() - t0, pg, "cuda")
     e2e_value = aggregate_rate(n * e2e_steps, world, e2e_s)
+    pcie = measure_pcie(torch, hbufs[1], hbufs[2], y, n, e2e_value / world)
     # correctness of the pipelined path: a fresh input through it equals the device result
     hbufs[0].copy_(x.cpu())
     z.ntt_host_many(tw, [hbufs[0].data_ptr()], z.FORWARD)
@@ -391,7 +392,8 @@ def run_zntt(args, rank, world, local):
         "e2e": {"value": e2e_value, "unit": "elements/s", "h2d_bytes_per_step": n * 32, "d2h_bytes_per_step": n * 32,
                 "steps": e2e_steps, "api": "zntt_ntt_host_many (pinned host vectors, copies overlapped across steps)",
                 "matches_device_result": ok,
-                "single_call_value": e2e_single, "single_call_api": "zntt_ntt_with_twiddles, one synchronous call"},
+                "single_call_value": e2e_single, "single_call_api": "zntt_ntt_with_twiddles, one synchronous call",
+                "pcie": pcie},
         "gpu_launches": args.steps * passes,
         "roofline": {"bound": "imad", "achieved": achieved, "peak": peak_modmul, "unit": "modmul/s",
                      "frac": achieved / peak_modmul, "traffic": traffic,
@@ -425,6 +427,44 @@ class TableCache:
     def close(self):
         for t in self.t.values():
             t.close()
+
+
+def measure_pcie(torch, h_in, h_out, d_src, n, e2e_per_gpu):
+    """Pinned host <-> device copy bandwidth of one step's vectors (n x 32 bytes), alone and with
+    both directions at once on two streams: the bound that the e2e path, which moves one
+    vector each way per step, cannot beat on this GPU.  Returns the GB/s figures, the duplex
+    bound in elements/s per GPU and the e2e fraction of it."""
+    d_dst = torch.empty_like(d_src)
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    nbytes = n * 32
+
+    def timed(copy_in, copy_out, reps=4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for st in (s_in, s_out):
+            st.wait_event(e0)
+        for _ in range(reps):
+            if copy_in:
+                with torch.cuda.stream(s_in):
+                    d_dst.copy_(h_in, non_blocking=True)
+            if copy_out:
+                with torch.cuda.stream(s_out):
+                    h_out.copy_(d_src, non_blocking=True)
+        for st in (s_in, s_out):
+            torch.cuda.current_stream().wait_stream(st)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e-3 / reps
+
+    timed(True, True, 1)  # warm-up
+    t_in, t_out, t_both = timed(True, False), timed(False, True), timed(True, True)
+    del d_dst
+    bound = n / t_both
+    return {"h2d_gbs": nbytes / t_in / 1e9, "d2h_gbs": nbytes / t_out / 1e9,
+            "duplex_gbs_each_way": nbytes / t_both / 1e9, "bound_elements_per_s": bound,
+            "e2e_frac_of_bound": e2e_per_gpu / bound,
+            "note": "torch copies of one n x 32-byte vector each way, pinned host memory, CUDA events"}
 
 
 def time_region(torch, stream, fn, steps):
