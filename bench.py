@@ -373,7 +373,8 @@ def run_zntt(args, rank, world, local):
                                                 cpu_sample=not args.no_cpu_baseline)
             extra["small_fields"] = run_small_config(z, torch, stream, steps=20, warmup=3,
                                                      cpu_sample=not args.no_cpu_baseline)
-            extra["fri_fold"] = run_fri_config(z, torch, stream, steps=20, warmup=3)
+            extra["fri_fold"] = run_fri_config(z, torch, stream, steps=20, warmup=3,
+                                               cpu_sample=not args.no_cpu_baseline)
     if pg:
         pg.barrier()
         pg.destroy_process_group()
@@ -690,7 +691,27 @@ def run_small_config(z, torch, stream, steps, warmup, log_n=24, cpu_sample=True)
     return out
 
 
-def run_fri_config(z, torch, stream, steps, warmup, log_n=24):
+def cpu_fri_sample(fid_name, log_sample=20):
+    """The oracle port's fold (the reference's literal loop: an inverse per element) and layer
+    commitment (hashPair + BLAKE3 Merkle tree) on one 2^log_sample layer, all host cores."""
+    workers = min(os.cpu_count() or 1, 64)
+    O, _ = cpu_oracle(native=True)
+    fid = {"bn254_fr": O.BN254_FR, "goldilocks": O.GOLDILOCKS}[fid_name]
+    n = 1 << log_sample
+    layer = O.random_elements(fid, 5, n)
+    alpha = O.random_elements(fid, 6, 1)[0]
+    t0 = time.perf_counter()
+    O.fri_fold(fid, layer, log_sample, alpha, workers=workers)
+    t_fold = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.fri_commit_layer(fid, layer, log_sample, workers=workers)
+    t_commit = time.perf_counter() - t0
+    return {"sample": f"one 2^{log_sample} layer: fold and commitment, oracle port on {workers} threads",
+            "fold_value": (n // 2) / t_fold, "fold_unit": "output elements/s",
+            "commit_hashes_per_s": (n - 1) / t_commit, "cores": workers, "kind": "port"}
+
+
+def run_fri_config(z, torch, stream, steps, warmup, log_n=24, cpu_sample=True):
     """FRI fold rounds (libs/fri/src/root.zig:396-403) on resident evaluations: one fold of a
     2^log_n layer, and the whole chain 2^log_n -> 2^10 sharing one table, for BN254-Fr and
     Goldilocks.  A fold reads the layer and the 1/(2x) table and writes half a layer."""
@@ -776,6 +797,7 @@ def run_fri_config(z, torch, stream, steps, warmup, log_n=24):
             "commit_note": "hashPair leaves + BLAKE3 Merkle tree, n - 1 single-block compressions; "
                            "the call copies the root to the host, inside the timed region",
             "prove_commit_ms": ms_prove, "prove_queries_ms": ms_queries,
+            "cpu_baseline": cpu_fri_sample(F.name) if cpu_sample else None,
             "prove_note": f"zntt_fri_commit_phase: {rounds} rounds of commit, root to the host, challenge "
                           f"callback, fold (2^{log_n} -> 2^10); zntt_fri_query_extract: 64 openings "
                           f"(pairs and Merkle paths of every round) to the host",
@@ -885,7 +907,8 @@ def run_single_config(args):
             r["unit"] = "elements/s"
             metric = "Goldilocks NTT elems/s at 2^24 (BabyBear beside it)"
         elif args.workload == "fri":
-            r = run_fri_config(z, torch, stream, steps=args.steps, warmup=args.warmup)
+            r = run_fri_config(z, torch, stream, steps=args.steps, warmup=args.warmup,
+                               cpu_sample=not args.no_cpu_baseline)
             r["value"] = r["fields"]["bn254_fr"]["fold_value"]
             r["unit"] = "output elements/s"
             metric = "BN254-Fr FRI fold output elems/s (2^24 -> 2^23; Goldilocks beside it)"
