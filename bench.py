@@ -684,6 +684,18 @@ def run_small_config(z, torch, stream, steps, warmup, log_n=24, cpu_sample=True)
              "hbm": {"achieved": moved / (ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                      "frac": moved / (ms * 1e-3) / 1e9 / hbm_peak, "bytes_per_transform": moved,
                      "peak_source": hbm_src}}
+        # Coset extension 2^(log_n - 2) -> 2^log_n (blowup 4, shift 7): inverse transform,
+        # coset scaling, zero tail, forward transform.
+        lin = log_n - 2
+        with z.DeviceTwiddles(F, lin, z.primitiveRootOfUnity(F, lin)) as ti, \
+                z.DeviceTwiddles(F, log_n, z.primitiveRootOfUnity(F, log_n)) as to:
+            shift = np.array([7, 0, 0, 0], dtype=np.uint64)
+            lde = lambda: z.coset_lde_device(ti, to, shift, x.data_ptr(), y.data_ptr(), stream=sptr)  # noqa: E731
+            for _ in range(warmup):
+                lde()
+            r["lde_ms"] = time_region(torch, stream, lde, steps) / steps
+        r["lde_note"] = (f"coset extension 2^{lin} -> 2^{log_n} (zntt_coset_lde_device; the call waits for "
+                         f"its stream)")
         if cpu_sample:
             r["cpu_baseline"] = cpu_small_sample(F, xs, log_n)
         out["fields"][F.name] = r

@@ -193,7 +193,9 @@ int zntt_batch_destroy(zntt_batch* b);
 
 /* One coset low-degree extension with plain per-pass launches:
  * d_out = ntt_{2^log_n}((intt_{2^log_in}(d_evals) zero-padded) . g^i), where
- * log_in / log_n are those of tw_in / tw_out. */
+ * log_in / log_n are those of tw_in / tw_out.  All four fields: with
+ * Goldilocks / BabyBear tables the shift is a nonzero canonical value in word 0
+ * and the call waits for its stream. */
 int zntt_coset_lde_device(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t shift[4],
                           const uint64_t* d_evals, uint64_t* d_out, void* stream);
 

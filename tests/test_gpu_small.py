@@ -167,14 +167,53 @@ def test_device_api_full_size(z):
             torch.cuda.empty_cache()
 
 
+@pytest.mark.parametrize("log_in,log_blowup", [(0, 1), (4, 2), (10, 1), (13, 2), (18, 2)])
+def test_coset_lde_matches_oracle(z, log_in, log_blowup):
+    """zntt_coset_lde_device with small-field tables against the oracle's composition
+    (inttWithTwiddles, zero padding, powers(shift) hadamard, nttWithTwiddles; the oracle's
+    zo_coset_lde), shift 7, one and several passes on either side."""
+    torch = pytest.importorskip("torch")
+    for F, fid in _fields(z):
+        log_out = log_in + log_blowup
+        x = _random(fid, 800 + log_in, 1 << log_in)
+        want = _canon(fid, O.coset_lde(fid, _slots(fid, x), log_in, log_blowup, _slots(fid, [7])[0], workers=WORKERS))
+        src = torch.from_numpy(x.view(np.int64).copy()).cuda()
+        out = torch.empty(1 << log_out, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        with z.DeviceTwiddles(F, log_in, z.primitiveRootOfUnity(F, log_in)) as ti, \
+                z.DeviceTwiddles(F, log_out, z.primitiveRootOfUnity(F, log_out)) as to:
+            z.coset_lde_device(ti, to, np.array([7, 0, 0, 0], dtype=np.uint64), src.data_ptr(), out.data_ptr())
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out.cpu().numpy().view(np.uint64), want, err_msg=f"{F.name} 2^{log_in}")
+
+
+def test_coset_lde_argument_checks(z):
+    """A shift that is not a nonzero canonical element, tables of two fields, and an output
+    overlapping the input are refused."""
+    torch = pytest.importorskip("torch")
+    F = z.GOLDILOCKS
+    buf = torch.zeros(1 << 12, dtype=torch.int64, device="cuda")
+    with z.DeviceTwiddles(F, 4, z.primitiveRootOfUnity(F, 4)) as t, \
+            z.DeviceTwiddles(F, 6, z.primitiveRootOfUnity(F, 6)) as t6, \
+            z.DeviceTwiddles(z.BABYBEAR, 6, z.primitiveRootOfUnity(z.BABYBEAR, 6)) as b6, \
+            z.DeviceTwiddles(z.BN254_FR, 6, z.primitiveRootOfUnity(z.BN254_FR, 6)) as w6:
+        for shift in ([0, 0, 0, 0], [F.modulus, 0, 0, 0], [5, 1, 0, 0]):
+            with pytest.raises(z.InvalidArgument):
+                z.coset_lde_device(t, t6, np.array(shift, dtype=np.uint64), buf.data_ptr(), buf[2048:].data_ptr())
+        for other in (b6, w6):
+            with pytest.raises(z.InvalidArgument):
+                z.coset_lde_device(t, other, np.array([7, 0, 0, 0], dtype=np.uint64), buf.data_ptr(),
+                                   buf[2048:].data_ptr())
+        with pytest.raises(z.InvalidArgument):
+            z.coset_lde_device(t, t6, np.array([7, 0, 0, 0], dtype=np.uint64), buf.data_ptr(), buf[8:].data_ptr())
+
+
 def test_small_tables_are_refused_by_256_bit_entry_points(z):
     torch = pytest.importorskip("torch")
     F = z.GOLDILOCKS
     buf = torch.zeros(1 << 12, dtype=torch.int64, device="cuda")
     with z.DeviceTwiddles(F, 4, z.primitiveRootOfUnity(F, 4)) as t, \
             z.DeviceTwiddles(F, 6, z.primitiveRootOfUnity(F, 6)) as t6:
-        with pytest.raises(z.UnsupportedField):
-            z.coset_lde_device(t, t6, z.to_montgomery(z.BN254_FR, 5), buf.data_ptr(), buf[2048:].data_ptr())
         with pytest.raises(z.UnsupportedField):
             z.poly_mul_device(t6, buf.data_ptr(), 3, buf[1024:].data_ptr(), 3, buf[2048:].data_ptr())
         with pytest.raises(z.UnsupportedField):

@@ -418,8 +418,9 @@ int zntt_coset_lde_device(const zntt_twiddles* tw_in, const zntt_twiddles* tw_ou
   if (!tw_in || !tw_out || !shift || !d_evals || !d_out) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
   Context& c = ctx();
   if (c.device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
-  if (is_small_table(tw_in) || is_small_table(tw_out))
-    return set_error(ZNTT_ERR_UNSUPPORTED_FIELD, "coset extensions take BN254-Fr or BLS12-381-Fr tables only");
+  if (is_small_table(tw_in) != is_small_table(tw_out))
+    return set_error(ZNTT_ERR_INVALID_ARGUMENT, "tables of different fields");
+  if (is_small_table(tw_in)) return small_coset_lde(tw_in, tw_out, shift, d_evals, d_out, stream);
   const TwEntry* ti = tw_of(tw_in);
   const TwEntry* to = tw_of(tw_out);
   if (ti->field != to->field) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "tables of different fields");

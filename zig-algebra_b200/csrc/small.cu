@@ -235,6 +235,19 @@ __global__ void small_powers_kernel(const uint64_t* __restrict__ pw, uint64_t c,
   }
 }
 
+// data[i] *= shift^i for i < count (< 2^30), the coset step of an extension,
+// from power tables of the shift in twiddle form (so the product of three
+// table entries is the twiddle form of shift^i, and its product with the
+// canonical data[i] is canonical).
+template <class SF>
+__global__ void small_coset_scale_kernel(const uint64_t* __restrict__ pw, uint64_t* __restrict__ data,
+                                         uint64_t count) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t v = SF::mul(__ldg(pw + (i & 1023)), __ldg(pw + 1024 + ((i >> 10) & 1023)));
+    data[i] = SF::mul(SF::mul(v, __ldg(pw + 2048 + (i >> 20))), data[i]);
+  }
+}
+
 // One FRI fold round (libs/fri/src/root.zig:396-403) on canonical values;
 // half_inv, alpha and the table g^-j / 2 are in twiddle form.
 template <class SF>
@@ -929,3 +942,72 @@ extern "C" int zntt_bit_reverse_small(uint64_t* data, size_t len) {
   zntt::clear_error();
   return zntt::small_bit_reverse(data, len);
 }
+
+namespace zntt {
+
+// The coset low-degree extension for a small field, the composition the
+// 256-bit path runs in its fused passes, as separate device steps: the
+// inverse transform of the 2^log_in evaluations into the head of d_out (with
+// 1/n), coefficient i times shift^i, the tail zeroed, and the forward
+// transform of d_out in place.
+int small_coset_lde(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t* shift,
+                    const uint64_t* d_evals, uint64_t* d_out, void* stream) {
+  const SmallTable* ti = reinterpret_cast<const SmallTable*>(tw_in);
+  const SmallTable* to = reinterpret_cast<const SmallTable*>(tw_out);
+  if (ti->field != to->field) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "tables of different fields");
+  if (ti->log_n > to->log_n) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "coset extension shrinks the vector");
+  if (ti->log_n > 30) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "coset extension of more than 2^30 evaluations");
+  const SmallHost& H = small_host(ti->field);
+  if (shift[1] || shift[2] || shift[3] || shift[0] >= H.p || shift[0] == 0)
+    return set_error(ZNTT_ERR_INVALID_ARGUMENT, "the shift must be a nonzero canonical element in word 0");
+  const uint64_t n_in = 1ull << ti->log_n, n_out = 1ull << to->log_n;
+  const char* eo = reinterpret_cast<const char*>(d_evals);
+  const char* oo = reinterpret_cast<const char*>(d_out);
+  if (oo < eo + n_in * 8 && eo < oo + n_out * 8) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "extension in place");
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+  std::vector<uint64_t> pw(3 * 1024);
+  uint64_t step = shift[0];
+  for (int t = 0; t < 3; t++) {
+    uint64_t cur = 1;
+    for (int i = 0; i < 1024; i++) {
+      pw[t * 1024 + i] = H.to_tw(cur);
+      cur = H.mul(cur, step);
+    }
+    step = H.pow(step, 1024);
+  }
+  void* d_pw = nullptr;
+  int rc = pool_get(pw.size() * 8, &d_pw);
+  if (rc) return rc;
+  void* scratch = nullptr;
+  const size_t sbytes = (size_t)8 << to->log_n;
+  rc = pool_get(sbytes, &scratch);
+  if (rc) {
+    pool_put(d_pw, pw.size() * 8);
+    return rc;
+  }
+  cudaError_t ce = cudaMemcpyAsync(d_pw, pw.data(), pw.size() * 8, cudaMemcpyHostToDevice, st);
+  if (ce == cudaSuccess) {
+    rc = small_run(ti, d_evals, d_out, nullptr, true, true, n_inverse_tw(H, ti->log_n), st);  // out of place
+    if (rc == ZNTT_OK) {
+      if (ti->field == kGoldilocksField)
+        small_coset_scale_kernel<Goldilocks><<<grid_for(n_in), 256, 0, st>>>((const uint64_t*)d_pw, d_out, n_in);
+      else
+        small_coset_scale_kernel<BabyBear><<<grid_for(n_in), 256, 0, st>>>((const uint64_t*)d_pw, d_out, n_in);
+      ce = cudaGetLastError();
+      if (ce == cudaSuccess && n_out > n_in) ce = cudaMemsetAsync(d_out + n_in, 0, (n_out - n_in) * 8, st);
+      if (ce == cudaSuccess) rc = small_run(to, d_out, d_out, (uint64_t*)scratch, false, false, 0, st);
+    }
+  }
+  // The power tables and the scratch return to the pool after the stream is done.
+  cudaError_t ce2 = cudaStreamSynchronize(st);
+  pool_put(d_pw, pw.size() * 8);
+  pool_put(scratch, sbytes);
+  if (rc) return rc;
+  if (ce == cudaSuccess) ce = ce2;
+  if (ce != cudaSuccess) return cuda_fail(ce, "coset extension");
+  return ZNTT_OK;
+}
+
+}  // namespace zntt
