@@ -363,3 +363,36 @@ def test_prove_config_checks(z):
             z.fri_prove(z.BN254_FR, pyref.Transcript(b"x"), 1, z.FriConfig(*args))
     with pytest.raises(z.InvalidArgument):
         z.fri_prove(z.BABYBEAR, pyref.Transcript(b"x"), 1, z.FriConfig(28, 20, 10, 2, 3))
+
+
+def test_extension_then_prove_goldilocks(z):
+    """A STARK prover's path over Goldilocks kept on the device: 2^16 evaluations extended to
+    2^20 (zntt_coset_lde_device, shift 1, so the result is the same polynomial on the larger
+    subgroup), then zig-fri's prove on the extension; the proof equals the oracle's (prove on
+    the oracle's own extension) and passes the restated verifier."""
+    import pyref
+    torch = _torch()
+    F, fid = _all(z)[2]
+    log_in, log_domain, log_final = 16, 20, 8
+    x = np.random.default_rng(990).integers(0, F.modulus, 1 << log_in, dtype=np.uint64)
+    src = torch.from_numpy(x.view(np.int64).copy()).cuda()
+    ext = torch.empty(1 << log_domain, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    with z.DeviceTwiddles(F, log_in, z.primitiveRootOfUnity(F, log_in)) as ti, \
+            z.DeviceTwiddles(F, log_domain, z.primitiveRootOfUnity(F, log_domain)) as to:
+        z.coset_lde_device(ti, to, np.array([1, 0, 0, 0], dtype=np.uint64), src.data_ptr(), ext.data_ptr())
+    torch.cuda.synchronize()
+    slots = O.elems(len(x))
+    slots[:, 0] = x
+    want_ext = O.coset_lde(fid, O.to_mont(fid, slots), log_in, log_domain - log_in, O.to_mont(fid, O.from_ints([1]))[0],
+                           workers=WORKERS)
+    np.testing.assert_array_equal(_from_dev(F, ext), want_ext)
+    rounds = log_domain - log_final
+    config = z.FriConfig(log_domain, log_in, log_final, log_in - rounds, 16)
+    label = b"lde then fri"
+    proof = z.fri_prove(F, pyref.Transcript(label), ext.data_ptr(), config)
+    want = O.fri_prove(fid, want_ext, log_domain, log_final, log_in - rounds, 16, pyref.Transcript(label),
+                       workers=WORKERS)
+    assert _proof_dict(proof) == want
+    assert pyref.fri_verify(O.MODULI[fid], O.element_bytes(fid), pyref.Transcript(label), want, log_domain,
+                            log_final, log_in - rounds, 16)
