@@ -257,6 +257,15 @@ int zntt_fri_fold_device(int field, const uint64_t* d_layer, uint32_t log_n, con
 int zntt_fri_commit_layer(int field, const uint64_t* d_layer, uint32_t log_n, uint8_t* d_nodes,
                           uint8_t* root_out, void* stream);
 
+/* One fold round followed by the commitment of the layer it makes, in one pass:
+ * the same results as zntt_fri_fold_device(field, d_layer, log_n, alpha, d_out,
+ * log_table) then zntt_fri_commit_layer(field, d_out, log_n - 1, d_nodes, root_out),
+ * with the new layer's leaves hashed by the threads that fold their values (proveOn's
+ * round r fold and round r + 1 commit, libs/fri/src/root.zig:372-403).  log_n >= 2;
+ * alpha must be a field element; the layer, d_out and d_nodes must not overlap. */
+int zntt_fri_fold_commit(int field, const uint64_t* d_layer, uint32_t log_n, const uint64_t alpha[4],
+                         uint64_t* d_out, uint32_t log_table, uint8_t* d_nodes, uint8_t* root_out, void* stream);
+
 /* The Fiat-Shamir challenge of FRI round `round`, computed by the caller's transcript
  * (proveOn's absorbBytes(root) then challengeFieldChecked, root.zig:386-388): writes alpha
  * in the field's scalar layout (Montgomery limbs below p; a small field's canonical value

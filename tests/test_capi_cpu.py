@@ -118,8 +118,9 @@ def test_poly_mul_contract_before_any_device_work(zntt, oracle):
 
 
 def test_fri_prover_loop_arguments_before_any_device_work(zntt):
-    """The commit phase and the query openings check Config.rounds' size rules
-    (libs/fri/src/root.zig:188-195), the field and their pointers before they look for a device."""
+    """The commit phase, the fused fold and commitment and the query openings check their sizes
+    (Config.rounds' rules, libs/fri/src/root.zig:188-195), the field, alpha and their pointers
+    before they look for a device."""
     F = zntt.BN254_FR
     never = lambda r, root: [0, 0, 0, 0]  # noqa: E731
     for log_domain, log_final in ((4, 4), (4, 5), (0, 0), (20, 13)):
@@ -136,6 +137,12 @@ def test_fri_prover_loop_arguments_before_any_device_work(zntt):
         zntt.fri_query_extract(F, 6, 2, [1] * 3, [16] * 3, [64])  # a position outside the domain
     with pytest.raises(zntt.InvalidArgument):
         zntt.fri_query_extract(F, 6, 2, [1] * 3, [16] * 3, [])  # no queries
+    with pytest.raises(zntt.InvalidArgument):
+        zntt.fri_fold_commit(F, 1 << 20, 1, [0, 0, 0, 0], 1 << 24, 1 << 28)  # nothing left to commit
+    with pytest.raises(zntt.InvalidArgument):
+        zntt.fri_fold_commit(F, 1 << 20, 6, [2**64 - 1] * 4, 1 << 24, 1 << 28)  # alpha >= p
+    with pytest.raises(zntt.UnsupportedField):
+        zntt.fri_fold_commit(zntt.Field(9, "bogus", 7, 1), 1 << 20, 6, [0, 0, 0, 0], 1 << 24, 1 << 28)
 
 
 def test_small_fields_host_side(zntt, oracle):

@@ -396,3 +396,41 @@ def test_extension_then_prove_goldilocks(z):
     assert _proof_dict(proof) == want
     assert pyref.fri_verify(O.MODULI[fid], O.element_bytes(fid), pyref.Transcript(label), want, log_domain,
                             log_final, log_in - rounds, 16)
+
+
+@pytest.mark.parametrize("log_n", [2, 3, 9, 10, 11, 14, 20])
+def test_fold_commit_equals_fold_then_commit(z, log_n):
+    """zntt_fri_fold_commit (a fold fused with the commitment of the layer it makes) equals
+    zntt_fri_fold_device followed by zntt_fri_commit_layer -- new layer, whole node array and
+    root -- on all four fields, on both sides of every launch boundary of the tree, with a
+    table shared with a larger first layer (log_table = log_n + 2)."""
+    torch = _torch()
+    for F, fid in _all(z):
+        n = 1 << log_n
+        layer = _to_dev(F, O.random_elements(fid, 1200 + log_n, n))
+        alpha = _scalar(F, O.random_elements(fid, 1300 + log_n, 1)[0])
+        half = (n // 2) * F.limbs
+        out_a, out_b = (torch.empty(half, dtype=torch.int64, device="cuda") for _ in range(2))
+        nodes_a, nodes_b = (torch.empty((n // 2) * 4, dtype=torch.int64, device="cuda") for _ in range(2))
+        torch.cuda.synchronize()
+        root_a = z.fri_fold_commit(F, layer.data_ptr(), log_n, alpha, out_a.data_ptr(), nodes_a.data_ptr(),
+                                   log_table=log_n + 2)
+        z.fri_fold(F, layer.data_ptr(), log_n, alpha, out_b.data_ptr(), log_table=log_n + 2)
+        root_b = z.fri_commit_layer(F, out_b.data_ptr(), log_n - 1, nodes_b.data_ptr())
+        torch.cuda.synchronize()
+        assert root_a == root_b, F.name
+        assert torch.equal(out_a, out_b), F.name
+        assert torch.equal(nodes_a, nodes_b), F.name
+
+
+def test_fold_commit_argument_checks(z):
+    torch = _torch()
+    F = z.BN254_FR
+    buf = torch.empty(1 << 14, dtype=torch.int64, device="cuda")
+    one = z.to_montgomery(F, 1)
+    with pytest.raises(z.InvalidArgument):  # the new layer overlaps the old one
+        z.fri_fold_commit(F, buf.data_ptr(), 6, one, buf[64:].data_ptr(), buf[8192:].data_ptr())
+    with pytest.raises(z.InvalidArgument):  # the nodes overlap the new layer
+        z.fri_fold_commit(F, buf.data_ptr(), 6, one, buf[4096:].data_ptr(), buf[4100:].data_ptr())
+    with pytest.raises(z.InvalidArgument):  # log_table below log_n
+        z.fri_fold_commit(F, buf.data_ptr(), 6, one, buf[4096:].data_ptr(), buf[8192:].data_ptr(), log_table=5)

@@ -218,6 +218,8 @@ def lib():
         L.zntt_poly_mul_device.argtypes = [vp, vp, sz, vp, sz, vp, vp]
         L.zntt_fri_domain_fill.argtypes = [i, ctypes.c_uint32, vp, vp]
         L.zntt_fri_fold_device.argtypes = [i, vp, ctypes.c_uint32, _U64P, vp, ctypes.c_uint32, vp]
+        L.zntt_fri_fold_commit.argtypes = [i, vp, ctypes.c_uint32, _U64P, vp, ctypes.c_uint32, vp, ctypes.c_char_p,
+                                           vp]
         L.zntt_fri_commit_phase.argtypes = [i, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(vp),
                                             ctypes.POINTER(vp), ctypes.c_char_p, FRI_CHALLENGE_FN, vp, vp]
         L.zntt_fri_query_extract.argtypes = [i, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(vp),
@@ -592,6 +594,17 @@ def fri_fold(F: Field, d_layer: int, log_n: int, alpha, d_out: int, log_table: i
     into 2^(log_n - 1); `alpha` in the field's scalar form (4 Montgomery limbs, or [value, 0, 0, 0])."""
     _ensure_init()
     _check(lib().zntt_fri_fold_device(F.id, d_layer, log_n, _root(alpha), d_out, log_table, stream or None))
+
+
+def fri_fold_commit(F: Field, d_layer: int, log_n: int, alpha, d_out: int, d_nodes: int, log_table: int = 0,
+                    stream: int = 0) -> bytes:
+    """One fold round of a device layer of 2^log_n evaluations into d_out and the commitment of
+    that new layer into d_nodes, in one pass (zntt_fri_fold_commit); returns the new layer's root."""
+    _ensure_init()
+    root = ctypes.create_string_buffer(32)
+    _check(lib().zntt_fri_fold_commit(F.id, d_layer, log_n, _root(alpha), d_out, log_table, d_nodes, root,
+                                      stream or None))
+    return root.raw
 
 
 def fri_commit_phase(F: Field, log_domain: int, log_final: int, d_layers, d_nodes, challenge,

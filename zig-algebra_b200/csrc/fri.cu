@@ -97,6 +97,19 @@ int fold_table(int field, uint32_t log_n, const uint4** out) {
 
 }  // namespace
 
+int wide_fold_params(int field, uint32_t log_table, const void** tab_out, uint32_t half_inv[8]) {
+  const uint4* tab = nullptr;
+  int rc = fold_table(field, log_table, &tab);
+  if (rc) return rc;
+  const HostField& F = host_field(field);
+  uint64_t two[4], hi[4];
+  F.from_u64(2, two);
+  F.inv(two, hi);
+  std::memcpy(half_inv, hi, 32);
+  *tab_out = tab;
+  return ZNTT_OK;
+}
+
 void fri_shutdown() {
   for (auto& kv : fold_tables())
     if (kv.second.d) cudaFree(kv.second.d);

@@ -881,6 +881,40 @@ int small_domain_fill(int field, uint32_t log_n, uint64_t* d_out, void* stream) 
   return small_powers(field, g[0], 1, d_out, 1ull << log_n, stream ? (cudaStream_t)stream : c.stream);
 }
 
+// The fold's constants for a small field: the resident table g^-j / 2 of the
+// subgroup of order 2^log_table (made on first use), 1/2 and alpha, all three
+// in twiddle form.
+int small_fold_params(int field, uint32_t log_table, const uint64_t* alpha, const uint64_t** tab_out,
+                      uint64_t* half_inv_tw, uint64_t* alpha_tw) {
+  const SmallHost& H = small_host(field);
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  auto& tabs = small_fold_tables();
+  const auto key = std::make_pair(field, log_table);
+  const uint64_t half_inv = H.inv(2);
+  auto it = tabs.find(key);
+  if (it != tabs.end()) {
+    *tab_out = it->second;
+  } else {
+    uint64_t g[4];
+    small_primitive_root(field, log_table, g);
+    const uint64_t count = 1ull << (log_table - 1);
+    uint64_t* tab = nullptr;
+    cudaError_t ce = cudaMalloc((void**)&tab, count * 8);
+    if (ce != cudaSuccess) return cuda_fail(ce, "fold table");
+    int rc = small_powers(field, H.inv(g[0]), H.to_tw(half_inv), tab, count, c.stream);
+    if (rc) {
+      cudaFree(tab);
+      return rc;
+    }
+    tabs[key] = tab;
+    *tab_out = tab;
+  }
+  *half_inv_tw = H.to_tw(half_inv);
+  *alpha_tw = H.to_tw(alpha[0] % H.p);
+  return ZNTT_OK;
+}
+
 int small_fri_fold(int field, const uint64_t* d_layer, uint32_t log_n, const uint64_t* alpha, uint64_t* d_out,
                    uint32_t log_table, void* stream) {
   const SmallHost& H = small_host(field);
@@ -895,28 +929,11 @@ int small_fri_fold(int field, const uint64_t* d_layer, uint32_t log_n, const uin
   Context& c = ctx();
   if (c.device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
   std::lock_guard<std::recursive_mutex> lock(c.mu);
-  auto& tabs = small_fold_tables();
-  const auto key = std::make_pair(field, log_table);
-  uint64_t* tab = nullptr;
-  auto it = tabs.find(key);
-  const uint64_t half_inv = H.inv(2);
-  if (it != tabs.end()) {
-    tab = it->second;
-  } else {
-    uint64_t g[4];
-    small_primitive_root(field, log_table, g);
-    const uint64_t count = 1ull << (log_table - 1);
-    cudaError_t ce = cudaMalloc((void**)&tab, count * 8);
-    if (ce != cudaSuccess) return cuda_fail(ce, "fold table");
-    int rc = small_powers(field, H.inv(g[0]), H.to_tw(half_inv), tab, count, c.stream);
-    if (rc) {
-      cudaFree(tab);
-      return rc;
-    }
-    tabs[key] = tab;
-  }
+  const uint64_t* tab = nullptr;
+  uint64_t hv = 0, av = 0;
+  int rc = small_fold_params(field, log_table, alpha, &tab, &hv, &av);
+  if (rc) return rc;
   cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
-  const uint64_t hv = H.to_tw(half_inv), av = H.to_tw(alpha[0] % H.p);
   const uint32_t stride = log_table - log_n;
   if (field == kGoldilocksField)
     small_fri_fold_kernel<Goldilocks><<<grid_for(half), 256, 0, st>>>(d_layer, d_out, tab, half, stride, hv, av);

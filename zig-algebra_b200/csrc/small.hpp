@@ -29,6 +29,11 @@ int small_ntt_device(const zntt_twiddles* tw, const uint64_t* d_src, uint64_t* d
 int small_domain_fill(int field, uint32_t log_n, uint64_t* d_out, void* stream);
 int small_fri_fold(int field, const uint64_t* d_layer, uint32_t log_n, const uint64_t* alpha, uint64_t* d_out,
                    uint32_t log_table, void* stream);
+int small_fold_params(int field, uint32_t log_table, const uint64_t* alpha, const uint64_t** tab_out,
+                      uint64_t* half_inv_tw, uint64_t* alpha_tw);
+// The 256-bit fields' fold constants (fri.cu): the resident table g^-j / 2 and 1/2
+// (Montgomery limbs as eight 32-bit words).
+int wide_fold_params(int field, uint32_t log_table, const void** tab_out, uint32_t half_inv[8]);
 int small_coset_lde(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t* shift,
                     const uint64_t* d_evals, uint64_t* d_out, void* stream);
 void small_shutdown();
