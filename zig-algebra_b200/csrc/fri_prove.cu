@@ -126,25 +126,18 @@ int zntt_fri_commit_phase(int field, uint32_t log_domain, uint32_t log_final, ui
   else two_adicity = host_field(field).two_adicity;
   if (log_domain > two_adicity) return set_error(ZNTT_ERR_ORDER_TOO_LARGE, "domain larger than the two-adicity");
   std::lock_guard<std::recursive_mutex> lock(c.mu);
-  // For the small fields round r's fold runs fused with round r + 1's commitment
-  // (zntt_fri_fold_commit): alpha_r is known once root r is, and the leaves of
-  // layer r + 1 are made from the values the fold computes.  The 256-bit fields
-  // run the two as separate launches, which measured faster for them (14 rounds
-  // from 2^24 BN254-Fr: 3.05 ms separate, 3.19 ms fused).  The last fold has no
-  // commitment after it.
-  const bool fuse = is_small_field(field);
+  // Round r's fold runs fused with round r + 1's commitment (zntt_fri_fold_commit):
+  // alpha_r is known once root r is, and the leaves of layer r + 1 are made from
+  // the values the fold computes.  The last fold has no commitment after it.
   uint64_t alpha[4] = {0, 0, 0, 0};
   for (uint32_t r = 0; r < rounds; r++) {
     uint8_t* root = roots_out + 32 * (size_t)r;
     const uint32_t log_n = log_domain - r;
     if (r == 0)
       rc = zntt_fri_commit_layer(field, d_layers[0], log_n, d_nodes[0], root, stream);  // waits for the root
-    else if (fuse)
+    else
       rc = zntt_fri_fold_commit(field, d_layers[r - 1], log_n + 1, alpha, d_layers[r], log_domain, d_nodes[r], root,
                                 stream);
-    else if ((rc = zntt_fri_fold_device(field, d_layers[r - 1], log_n + 1, alpha, d_layers[r], log_domain, stream)) ==
-             ZNTT_OK)
-      rc = zntt_fri_commit_layer(field, d_layers[r], log_n, d_nodes[r], root, stream);
     if (rc) return rc;
     for (int k = 0; k < 4; k++) alpha[k] = 0;
     const int cs = challenge(user, r, root, alpha);
