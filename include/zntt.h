@@ -269,7 +269,10 @@ int zntt_fri_fold_commit(int field, const uint64_t* d_layer, uint32_t log_n, con
 /* The Fiat-Shamir challenge of FRI round `round`, computed by the caller's transcript
  * (proveOn's absorbBytes(root) then challengeFieldChecked, root.zig:386-388): writes alpha
  * in the field's scalar layout (Montgomery limbs below p; a small field's canonical value
- * in word 0, the other words zero) and returns 0, or nonzero to stop the phase. */
+ * in word 0, the other words zero) and returns 0, or nonzero to stop the phase.  It runs on
+ * the thread that called zntt_fri_commit_phase while that call holds the library's lock:
+ * it may call the library from that thread, but must not wait for another thread that
+ * does. */
 typedef int (*zntt_fri_challenge_fn)(void* user, uint32_t round, const uint8_t root[32], uint64_t alpha_out[4]);
 
 /* The commit phase of proveOn (libs/fri/src/root.zig:372-403) on resident layers:
