@@ -381,3 +381,15 @@ def test_fri_proof_fixture_oracle_and_verifier():
                 x = bad["residual"][0]
                 bad["residual"][0] = ("%02x" % (int(x[:2], 16) ^ 1)) + x[2:]
             assert not pyref.fri_verify(p, nb, pyref.Transcript(label), _proof_bytes(bad, cfg), *args), where
+
+
+@pytest.mark.parametrize("fname", ["goldilocks", "babybear"])
+def test_small_field_coset_lde_vs_pure_python(fname):
+    """The oracle's coset extension over the small fields (the checker of the device's
+    small-field zntt_coset_lde_device) against pyref's independent composition."""
+    f = FIELD_IDS[fname]
+    p = O.MODULI[f]
+    for log_in, log_blowup, shift in ((0, 1, 7), (3, 2, 7), (6, 1, 31), (8, 2, 1)):
+        vals = pyref.random_field_values(p, 40 + log_in, 1 << log_in)
+        got = _canon_ints(f, O.coset_lde(f, _mont_of(f, vals), log_in, log_blowup, _mont_of(f, [shift])[0]))
+        assert got == pyref.coset_lde(vals, log_blowup, shift, p), (log_in, log_blowup, shift)
