@@ -792,6 +792,26 @@ def run_fri_config(z, torch, stream, steps, warmup, log_n=24, cpu_sample=True):
         ms_one = time_region(torch, stream, one, steps) / steps
         ms_chain = time_region(torch, stream, chain, steps) / steps
         ms_commit = time_region(torch, stream, commit, steps) / steps
+        # Row commitment of 8 columns of 2^(log_n - 2) rows (MerkleTree.init over rows, a trace
+        # commitment): ceil(8 * NB / 64) compressions per row plus the tree's rows - 1.
+        rows_log, ncol = log_n - 2, 8
+        rows = 1 << rows_log
+        cols = [torch.empty(rows * F.limbs, dtype=torch.int64, device="cuda") for _ in range(ncol)]
+        for c_i, col in enumerate(cols):
+            if F.limbs == 4:
+                z.random_elements(F, 200 + c_i, col.data_ptr(), rows, stream=sptr)
+            else:
+                col.copy_(torch.from_numpy(np.random.default_rng(200 + c_i).integers(
+                    0, F.modulus, rows, dtype=np.uint64).view(np.int64)))
+        rnodes = torch.empty((2 * rows) * 4, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        col_ptrs = [c_.data_ptr() for c_ in cols]
+        rcommit = lambda: z.merkle_commit_rows(F, col_ptrs, rows_log, rnodes.data_ptr(), stream=sptr)  # noqa: E731
+        for _ in range(warmup):
+            rcommit()
+        ms_rows = time_region(torch, stream, rcommit, steps) / steps
+        rows_compressions = rows * -(-ncol * ew // 64) + rows - 1
+        del cols, rnodes
         layer_copy = layer.clone()  # the commit phase folds into bufs; layer 0 is only read
         for _ in range(2):
             prove()
@@ -814,6 +834,10 @@ def run_fri_config(z, torch, stream, steps, warmup, log_n=24, cpu_sample=True):
                            "the call copies the root to the host, inside the timed region",
             "prove_commit_ms": ms_prove, "prove_queries_ms": ms_queries,
             "cpu_baseline": cpu_fri_sample(F.name) if cpu_sample else None,
+            "rows_commit": {"columns": ncol, "rows": rows, "ms": ms_rows, "compressions": rows_compressions,
+                            "compressions_per_s": rows_compressions / (ms_rows * 1e-3),
+                            "frac_of_probe": rows_compressions / (ms_rows * 1e-3) / b3_peak,
+                            "note": "zntt_merkle_commit_rows: MerkleTree.init over the rows of the columns"},
             "prove_note": f"zntt_fri_commit_phase: {rounds} rounds of commit, root to the host, challenge "
                           f"callback, fold (2^{log_n} -> 2^10); zntt_fri_query_extract: 64 openings "
                           f"(pairs and Merkle paths of every round) to the host",

@@ -257,6 +257,17 @@ int zntt_fri_fold_device(int field, const uint64_t* d_layer, uint32_t log_n, con
 int zntt_fri_commit_layer(int field, const uint64_t* d_layer, uint32_t log_n, uint8_t* d_nodes,
                           uint8_t* root_out, void* stream);
 
+/* MerkleTree.init (libs/merkle/src/merkle_tree.zig:70-103) over the rows of num_columns
+ * device columns of 2^log_n elements each (the commitment of a prover's extended trace
+ * columns): leaf i = BLAKE3(toBytes(col_0[i]) || ... || toBytes(col_{m-1}[i])), the row
+ * serialized in column order the way hashPair serializes a pair; d_nodes (2^(log_n+1)
+ * digests of 32 bytes, 16-byte aligned) receives node 0 = zero, node 1 = the root,
+ * node 2^log_n + i = leaf i.  Rows of at most 1024 bytes (32 columns of a 256-bit field,
+ * 128 of Goldilocks, 256 of BabyBear); log_n <= 30.  root_out as in
+ * zntt_fri_commit_layer. */
+int zntt_merkle_commit_rows(int field, const uint64_t* const* d_columns, uint32_t num_columns, uint32_t log_n,
+                            uint8_t* d_nodes, uint8_t* root_out, void* stream);
+
 /* One fold round followed by the commitment of the layer it makes, in one pass:
  * the same results as zntt_fri_fold_device(field, d_layer, log_n, alpha, d_out,
  * log_table) then zntt_fri_commit_layer(field, d_out, log_n - 1, d_nodes, root_out),

@@ -84,6 +84,7 @@ def load(path: str | None = None):
     lib.zo_random_elements.argtypes = [i, ctypes.c_char_p, _U64P, sz]
     lib.zo_powers.argtypes = [i, _U64P, _U64P, sz]
     lib.zo_coset_lde.argtypes = [i, _U64P, sz, sz, _U64P, _U64P, i]
+    lib.zo_merkle_commit_rows.argtypes = [i, ctypes.POINTER(_U64P), sz, sz, ctypes.c_void_p, i]
     lib.zo_dft_points.argtypes = [i, _U64P, sz, _U64P, _U64P, sz, _U64P, i]
     lib.zo_poly_mul.argtypes = [i, _U64P, sz, _U64P, sz, sz, _U64P, ctypes.POINTER(ctypes.c_int64), i]
     lib.zo_poly_eval.argtypes = [i, _U64P, sz, _U64P, sz, _U64P, i]
@@ -395,3 +396,15 @@ def fri_prove(field: int, evals: np.ndarray, log_domain: int, log_final: int, lo
     return {"roots": roots, "residual": residual,
             "queries": [{"pair_index": e0, "values": values[q], "paths": paths[q]} for q, e0 in enumerate(positions)],
             "log_domain": log_domain, "log_final": log_final, "log_residual_degree": log_residual}
+
+
+def merkle_commit_rows(field: int, columns: list, log_n: int, workers: int = 1) -> np.ndarray:
+    """MerkleTree.init (libs/merkle/src/merkle_tree.zig:70-103) over the 2^log_n rows of the
+    columns (Montgomery slots): leaf i = BLAKE3 of the row's toBytes concatenated in column
+    order.  A (2^(log_n+1), 32) uint8 array of node digests, row 1 the root, row 0 zero."""
+    cols = [np.ascontiguousarray(c) for c in columns]
+    ptrs = (_U64P * len(cols))(*[c.ctypes.data_as(_U64P) for c in cols])
+    nodes = np.zeros((2 << log_n, 32), dtype=np.uint8)
+    st = load().zo_merkle_commit_rows(field, ptrs, len(cols), log_n, nodes.ctypes.data, workers)
+    assert st == OK, st
+    return nodes

@@ -1328,4 +1328,38 @@ int zo_fri_commit_layer(int field, const uint64_t* layer, size_t log_n, uint8_t*
   });
 }
 
+// MerkleTree.init (libs/merkle/src/merkle_tree.zig:70-103) over rows of columns:
+// leaf i = BLAKE3(toBytes(col_0[i]) || ... || toBytes(col_{m-1}[i])) -- the row
+// serialized the way hashPair serializes a pair -- for 2^log_n rows (a power of
+// two, so no padding leaves), then the same heap-ordered levels as above:
+// nodes[n + i] = leaf i, nodes[1] the root, nodes[0] zero.  Rows of at most
+// 1024 bytes (one BLAKE3 chunk).
+int zo_merkle_commit_rows(int field, const uint64_t* const* cols, size_t num_cols, size_t log_n, uint8_t* nodes,
+                          int workers) {
+  return dispatch(field, [&](const auto& F) -> int {
+    constexpr int N = sizeof(F.P) / sizeof(uint64_t);
+    const size_t nb = (size_t)(F.BITS + 7) / 8, n = (size_t)1 << log_n;
+    if (num_cols == 0 || num_cols * nb > 1024) return ZO_LENGTH_MISMATCH;
+    std::memset(nodes, 0, 32);
+    parallel_for(n, workers, [&](size_t lo, size_t hi) {
+      std::vector<uint8_t> row(num_cols * nb);
+      for (size_t i = lo; i < hi; i++) {
+        for (size_t c = 0; c < num_cols; c++) {
+          uint64_t m[N], v[N];
+          load<N>(cols[c] + 4 * i, m);
+          F.from_mont(m, v);
+          for (size_t k = 0; k < nb; k++) row[c * nb + k] = (uint8_t)(v[k / 8] >> (8 * (k % 8)));
+        }
+        b3_hash(row.data(), row.size(), nodes + 32 * (n + i));
+      }
+    });
+    for (size_t w = n / 2; w >= 1; w /= 2) {
+      parallel_for(w, w >= 4096 ? workers : 1, [&](size_t lo, size_t hi) {
+        for (size_t i = w + lo; i < w + hi; i++) b3_hash(nodes + 32 * (2 * i), 64, nodes + 32 * i);
+      });
+    }
+    return ZO_OK;
+  });
+}
+
 }  // extern "C"

@@ -24,6 +24,9 @@ Two kinds of fixture:
      fields: seeded factors of several lengths, trailing zero coefficients
      (normalized away), a zero factor, constants, and max_degree cases that
      fit exactly or raise DegreeTooLarge.
+   * merkle_rows.json -- row commitments (MerkleTree.init over the rows of several columns,
+     each row's toBytes values concatenated) for all four fields, rows of one block up to
+     one full 1024-byte chunk.
    * fri_proof.json -- the reference's transcript known answer (four Goldilocks
      challenges from Transcript.init("wire-compat"), libs/fri/src/root.zig, copied as
      data and reproduced by pyref.Transcript) and whole FRI proofs of pyref.fri_prove
@@ -245,6 +248,23 @@ def fri_proof_cases(ref: str) -> dict:
     return {"transcript_kat": kat, "config": cfg, "cases": cases}
 
 
+def merkle_rows_cases() -> dict:
+    """Row commitments (pyref.merkle_commit_rows: MerkleTree.init over rows of columns) for
+    seeded columns of all four fields, with rows of one block, several blocks and exactly one
+    chunk (1024 bytes)."""
+    cases = []
+    for q, (name, p, nb) in enumerate(FRI_FIELDS):
+        for m, log_n in ((1, 3), (2, 4), (3, 2), (5, 5), (1024 // nb, 2)):
+            cols = [pyref.random_field_values(p, 1500 + 37 * q + 7 * m + c, 1 << log_n) for c in range(m)]
+            nodes = pyref.merkle_commit_rows(cols, nb)
+            case = {"field": name, "columns": m, "log_n": log_n, "values": [[hex(v) for v in c] for c in cols],
+                    "root": nodes[1].hex()}
+            if log_n <= 4:
+                case["nodes"] = [x.hex() for x in nodes[1:]]
+            cases.append(case)
+    return {"cases": cases}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -256,6 +276,7 @@ def main() -> None:
     json.dump(poly_cases(), open(os.path.join(HERE, "poly_mul.json"), "w"), indent=1)
     json.dump(fri_commit_cases(args.reference), open(os.path.join(HERE, "fri_commit.json"), "w"), indent=1)
     json.dump(fri_proof_cases(args.reference), open(os.path.join(HERE, "fri_proof.json"), "w"), indent=1)
+    json.dump(merkle_rows_cases(), open(os.path.join(HERE, "merkle_rows.json"), "w"), indent=1)
     print("fixtures written to", HERE)
 
 

@@ -400,3 +400,22 @@ def fri_verify(p: int, num_bytes: int, transcript: Transcript, proof: dict, log_
                 return False
             e = j
     return True
+
+
+def merkle_commit_rows(columns: list[list[int]], num_bytes: int) -> list[bytes]:
+    """MerkleTree.init (libs/merkle/src/merkle_tree.zig:70-103) over the rows of equal-length
+    columns: leaf i = BLAKE3 of toBytes(col_0[i]) || ... || toBytes(col_{m-1}[i]), leaf count
+    padded to a power of two with BLAKE3 of the empty string, nodes[i] = BLAKE3(nodes[2i] ||
+    nodes[2i+1]).  Returns nodes[0 .. 2 * leaf_count) with nodes[0] all zero."""
+    n = len(columns[0])
+    count = 1
+    while count < n:
+        count *= 2
+    nodes = [bytes(32)] * (2 * count)
+    for i in range(n):
+        nodes[count + i] = blake3(b"".join(to_bytes(col[i], num_bytes) for col in columns))
+    for i in range(n, count):
+        nodes[count + i] = blake3(b"")
+    for i in range(count - 1, 0, -1):
+        nodes[i] = blake3(nodes[2 * i] + nodes[2 * i + 1])
+    return nodes

@@ -434,3 +434,51 @@ def test_fold_commit_argument_checks(z):
         z.fri_fold_commit(F, buf.data_ptr(), 6, one, buf[4096:].data_ptr(), buf[4100:].data_ptr())
     with pytest.raises(z.InvalidArgument):  # log_table below log_n
         z.fri_fold_commit(F, buf.data_ptr(), 6, one, buf[4096:].data_ptr(), buf[8192:].data_ptr(), log_table=5)
+
+
+def test_row_commitment_matches_fixture_and_oracle(z):
+    """zntt_merkle_commit_rows (MerkleTree.init over the rows of device columns) against the
+    pure-Python fixture and the oracle's whole node arrays: all four fields, 1 to the maximum
+    number of columns (one 1024-byte chunk per row), on both sides of the launch boundaries."""
+    import json
+    torch = _torch()
+    d = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "merkle_rows.json")))
+    names = {F.name: (F, fid) for F, fid in _all(z)}
+    for c in d["cases"]:
+        F, fid = names[c["field"]]
+        cols = [_to_dev(F, O.to_mont(fid, O.from_ints([int(v, 16) for v in col]))) for col in c["values"]]
+        nodes = torch.zeros((2 << c["log_n"]) * 4, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        root = z.merkle_commit_rows(F, [t.data_ptr() for t in cols], c["log_n"], nodes.data_ptr())
+        assert root.hex() == c["root"], (c["field"], c["columns"], c["log_n"])
+        if "nodes" in c:
+            got = nodes.cpu().numpy().view(np.uint8).reshape(-1, 32)
+            assert [x.tobytes().hex() for x in got[1:]] == c["nodes"]
+    for F, fid in _all(z):
+        nb = O.element_bytes(fid)
+        for m, log_n in ((1, 0), (1, 9), (3, 10), (8, 13), (1024 // nb, 12), (2, 16)):
+            host = [O.random_elements(fid, 1700 + 13 * m + c, 1 << log_n) for c in range(m)]
+            want = O.merkle_commit_rows(fid, host, log_n, workers=WORKERS)
+            cols = [_to_dev(F, h) for h in host]
+            nodes = torch.zeros((2 << log_n) * 4, dtype=torch.int64, device="cuda")
+            torch.cuda.synchronize()
+            z.merkle_commit_rows(F, [t.data_ptr() for t in cols], log_n, nodes.data_ptr())
+            torch.cuda.synchronize()
+            np.testing.assert_array_equal(nodes.cpu().numpy().view(np.uint8).reshape(-1, 32)[1:], want[1:],
+                                          err_msg=f"{F.name} {m} columns 2^{log_n}")
+
+
+def test_row_commitment_argument_checks(z):
+    torch = _torch()
+    F = z.BN254_FR
+    buf = torch.empty(1 << 14, dtype=torch.int64, device="cuda")
+    col = buf.data_ptr()
+    nodes = buf[8192:].data_ptr()
+    with pytest.raises(z.InvalidArgument):  # 33 columns of 32 bytes exceed one chunk
+        z.merkle_commit_rows(F, [col] * 33, 4, nodes)
+    with pytest.raises(z.InvalidArgument):
+        z.merkle_commit_rows(F, [col, 0], 4, nodes)
+    with pytest.raises(z.InvalidArgument):
+        z.merkle_commit_rows(F, [], 4, nodes)
+    with pytest.raises(z.InvalidArgument):  # the nodes overlap the column
+        z.merkle_commit_rows(F, [col], 6, buf[64:].data_ptr())

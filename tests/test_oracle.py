@@ -393,3 +393,17 @@ def test_small_field_coset_lde_vs_pure_python(fname):
         vals = pyref.random_field_values(p, 40 + log_in, 1 << log_in)
         got = _canon_ints(f, O.coset_lde(f, _mont_of(f, vals), log_in, log_blowup, _mont_of(f, [shift])[0]))
         assert got == pyref.coset_lde(vals, log_blowup, shift, p), (log_in, log_blowup, shift)
+
+
+def test_row_commitment_fixture():
+    """The oracle's row commitment (MerkleTree.init over rows, libs/merkle/src/merkle_tree.zig:
+    70-103) against the pure-Python one in merkle_rows.json, all four fields, rows of one block
+    to one full chunk."""
+    d = json.load(open(os.path.join(GOLDEN, "merkle_rows.json")))
+    for c in d["cases"]:
+        f = FIELD_IDS[c["field"]]
+        cols = [_mont_of(f, [int(v, 16) for v in col]) for col in c["values"]]
+        nodes = O.merkle_commit_rows(f, cols, c["log_n"], workers=4)
+        assert nodes[1].tobytes().hex() == c["root"], (c["field"], c["columns"])
+        if "nodes" in c:
+            assert [x.tobytes().hex() for x in nodes[1:]] == c["nodes"]

@@ -218,6 +218,8 @@ def lib():
         L.zntt_poly_mul_device.argtypes = [vp, vp, sz, vp, sz, vp, vp]
         L.zntt_fri_domain_fill.argtypes = [i, ctypes.c_uint32, vp, vp]
         L.zntt_fri_fold_device.argtypes = [i, vp, ctypes.c_uint32, _U64P, vp, ctypes.c_uint32, vp]
+        L.zntt_merkle_commit_rows.argtypes = [i, ctypes.POINTER(vp), ctypes.c_uint32, ctypes.c_uint32, vp,
+                                              ctypes.c_char_p, vp]
         L.zntt_fri_fold_commit.argtypes = [i, vp, ctypes.c_uint32, _U64P, vp, ctypes.c_uint32, vp, ctypes.c_char_p,
                                            vp]
         L.zntt_fri_commit_phase.argtypes = [i, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(vp),
@@ -749,6 +751,17 @@ def fri_prove(F: Field, transcript, d_evals: int, config: FriConfig, stream: int
                                       stream)
     queries = [{"pair_index": e0, "values": values[q], "paths": paths[q]} for q, e0 in enumerate(positions)]
     return FriProof(roots, residual, queries, config.log_domain, config.log_final, config.log_residual_degree)
+
+
+def merkle_commit_rows(F: Field, d_columns, log_n: int, d_nodes: int, stream: int = 0) -> bytes:
+    """MerkleTree.init over the 2^log_n rows of device columns (zntt_merkle_commit_rows): leaf i
+    hashes the row's toBytes values in column order; d_nodes receives 2^(log_n+1) digests of 32
+    bytes in heap order.  Returns the root."""
+    _ensure_init()
+    cols = (ctypes.c_void_p * max(len(d_columns), 1))(*d_columns)
+    root = ctypes.create_string_buffer(32)
+    _check(lib().zntt_merkle_commit_rows(F.id, cols, len(d_columns), log_n, d_nodes, root, stream or None))
+    return root.raw
 
 
 def fri_commit_layer(F: Field, d_layer: int, log_n: int, d_nodes: int, stream: int = 0) -> bytes:
