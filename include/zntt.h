@@ -268,6 +268,15 @@ int zntt_fri_commit_layer(int field, const uint64_t* d_layer, uint32_t log_n, ui
 int zntt_merkle_commit_rows(int field, const uint64_t* const* d_columns, uint32_t num_columns, uint32_t log_n,
                             uint8_t* d_nodes, uint8_t* root_out, void* stream);
 
+/* Openings of a row commitment (MerkleTree.prove, libs/merkle/src/merkle_tree.zig:206-233)
+ * for num_queries rows i < 2^log_n of the columns committed by zntt_merkle_commit_rows
+ * (d_nodes its node array): values_out + q * num_columns * NB receives row positions[q]'s
+ * toBytes values in column order, paths_out + q * log_n * 32 its log_n sibling digests
+ * from the leaf level up.  Host outputs; the call waits for them. */
+int zntt_merkle_open_rows(int field, const uint64_t* const* d_columns, uint32_t num_columns, uint32_t log_n,
+                          const uint8_t* d_nodes, const uint64_t* positions, size_t num_queries, uint8_t* values_out,
+                          uint8_t* paths_out, void* stream);
+
 /* One fold round followed by the commitment of the layer it makes, in one pass:
  * the same results as zntt_fri_fold_device(field, d_layer, log_n, alpha, d_out,
  * log_table) then zntt_fri_commit_layer(field, d_out, log_n - 1, d_nodes, root_out),

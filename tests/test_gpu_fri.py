@@ -482,3 +482,27 @@ def test_row_commitment_argument_checks(z):
         z.merkle_commit_rows(F, [], 4, nodes)
     with pytest.raises(z.InvalidArgument):  # the nodes overlap the column
         z.merkle_commit_rows(F, [col], 6, buf[64:].data_ptr())
+
+
+def test_row_openings_match_oracle_and_verify(z):
+    """zntt_merkle_open_rows: each opened row equals the columns' toBytes at that row, each path
+    equals the oracle tree's siblings (MerkleTree.prove, libs/merkle/src/merkle_tree.zig:206-233)
+    and authenticates the row's hash against the root; all four fields."""
+    torch = _torch()
+    for F, fid in _all(z):
+        for m, log_n in ((1, 0), (3, 11), (8, 14)):
+            host = [O.random_elements(fid, 1900 + 7 * m + c, 1 << log_n) for c in range(m)]
+            tree = O.merkle_commit_rows(fid, host, log_n, workers=WORKERS)
+            cols = [_to_dev(F, h) for h in host]
+            nodes = torch.empty((2 << log_n) * 4, dtype=torch.int64, device="cuda")
+            torch.cuda.synchronize()
+            root = z.merkle_commit_rows(F, [t.data_ptr() for t in cols], log_n, nodes.data_ptr())
+            positions = np.random.default_rng(log_n + m).integers(0, 1 << log_n, 9, dtype=np.uint64)
+            rows, paths = z.merkle_open_rows(F, [t.data_ptr() for t in cols], log_n, nodes.data_ptr(), positions)
+            byte_cols = [O.to_bytes(fid, h) for h in host]
+            for q, i in enumerate(int(p) for p in positions):
+                assert rows[q] == b"".join(bc[i] for bc in byte_cols), (F.name, m, q)
+                assert paths[q] == [tree[((1 << log_n) + i >> k) ^ 1].tobytes() for k in range(log_n)]
+                assert _verify_path(root, i, rows[q], paths[q]), (F.name, m, q)
+    with pytest.raises(z.InvalidArgument):  # a row outside the commitment
+        z.merkle_open_rows(z.GOLDILOCKS, [1], 4, 16, [16])

@@ -220,6 +220,8 @@ def lib():
         L.zntt_fri_fold_device.argtypes = [i, vp, ctypes.c_uint32, _U64P, vp, ctypes.c_uint32, vp]
         L.zntt_merkle_commit_rows.argtypes = [i, ctypes.POINTER(vp), ctypes.c_uint32, ctypes.c_uint32, vp,
                                               ctypes.c_char_p, vp]
+        L.zntt_merkle_open_rows.argtypes = [i, ctypes.POINTER(vp), ctypes.c_uint32, ctypes.c_uint32, vp, _U64P, sz,
+                                            ctypes.c_char_p, ctypes.c_char_p, vp]
         L.zntt_fri_fold_commit.argtypes = [i, vp, ctypes.c_uint32, _U64P, vp, ctypes.c_uint32, vp, ctypes.c_char_p,
                                            vp]
         L.zntt_fri_commit_phase.argtypes = [i, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(vp),
@@ -762,6 +764,25 @@ def merkle_commit_rows(F: Field, d_columns, log_n: int, d_nodes: int, stream: in
     root = ctypes.create_string_buffer(32)
     _check(lib().zntt_merkle_commit_rows(F.id, cols, len(d_columns), log_n, d_nodes, root, stream or None))
     return root.raw
+
+
+def merkle_open_rows(F: Field, d_columns, log_n: int, d_nodes: int, positions, stream: int = 0):
+    """Openings of a row commitment (zntt_merkle_open_rows): returns (rows, paths) with rows[q]
+    the toBytes values of row positions[q] in column order and paths[q] its sibling digests,
+    leaf level first."""
+    _ensure_init()
+    nb = _num_bytes(F)
+    pos = np.ascontiguousarray(np.asarray(positions, dtype=np.uint64))
+    nq, m = len(pos), len(d_columns)
+    cols = (ctypes.c_void_p * max(m, 1))(*d_columns)
+    vals = ctypes.create_string_buffer(max(nq * m * nb, 1))
+    paths = ctypes.create_string_buffer(max(nq * log_n * 32, 1))
+    _check(lib().zntt_merkle_open_rows(F.id, cols, m, log_n, d_nodes, pos.ctypes.data_as(_U64P) if nq else None, nq,
+                                       vals, paths, stream or None))
+    vraw, praw = vals.raw, paths.raw
+    rows = [vraw[q * m * nb:(q + 1) * m * nb] for q in range(nq)]
+    out = [[praw[(q * log_n + k) * 32:(q * log_n + k + 1) * 32] for k in range(log_n)] for q in range(nq)]
+    return rows, out
 
 
 def fri_commit_layer(F: Field, d_layer: int, log_n: int, d_nodes: int, stream: int = 0) -> bytes:

@@ -74,6 +74,31 @@ __global__ void query_kernel(QueryLayers L, const uint64_t* __restrict__ pos, ui
   }
 }
 
+// Openings of a row commitment (MerkleTree.prove over zntt_merkle_commit_rows'
+// tree): one thread per query writes row i's toBytes values in column order and
+// the log_n siblings of leaf i from the leaf level up.
+struct RowColumns {
+  const void* col[256];
+};
+
+template <int FIELD>
+__global__ void open_rows_kernel(RowColumns C, uint32_t m, uint32_t log_n, const uint4* __restrict__ nodes,
+                                 const uint64_t* __restrict__ pos, uint32_t nq, uint32_t* __restrict__ values,
+                                 uint4* __restrict__ paths) {
+  constexpr uint32_t kWords = (FIELD == kBn254Fr || FIELD == kBls12381Fr) ? 8 : (FIELD == kGoldilocksField ? 2 : 1);
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nq) return;
+  const uint64_t i = pos[q];
+  uint32_t* v = values + (uint64_t)q * m * kWords;
+  for (uint32_t c = 0; c < m; c++) element_words<FIELD>(C.col[c], i, v + c * kWords);
+  uint4* out = paths + 2 * (uint64_t)q * log_n;
+  uint64_t p = (1ull << log_n) + i;
+  for (uint32_t level = 0; level < log_n; level++, p >>= 1) {
+    out[2 * level] = nodes[2 * (p ^ 1)];
+    out[2 * level + 1] = nodes[2 * (p ^ 1) + 1];
+  }
+}
+
 uint32_t element_bytes(int field) {
   return is_small_field(field) ? (field == kGoldilocksField ? 8u : 4u) : 32u;
 }
@@ -223,3 +248,69 @@ int zntt_fri_query_extract(int field, uint32_t log_domain, uint32_t rounds, cons
 }
 
 }  // extern "C"
+
+extern "C" int zntt_merkle_open_rows(int field, const uint64_t* const* d_columns, uint32_t num_columns,
+                                     uint32_t log_n, const uint8_t* d_nodes, const uint64_t* positions,
+                                     size_t num_queries, uint8_t* values_out, uint8_t* paths_out, void* stream) {
+  clear_error();
+  int rc = check_field_id(field);
+  if (rc) return rc;
+  const uint32_t nb = element_bytes(field);
+  if (!d_columns || !d_nodes || !positions || !values_out || (!paths_out && log_n > 0))
+    return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
+  if (num_columns == 0 || num_columns * nb > 1024)
+    return set_error(ZNTT_ERR_INVALID_ARGUMENT, "rows of 1 .. 1024 bytes (one BLAKE3 chunk)");
+  if (log_n > 30) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "at most 2^30 rows");
+  if (num_queries == 0 || num_queries > (1u << 20)) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "1 .. 2^20 queries");
+  if (reinterpret_cast<uintptr_t>(d_nodes) % 16)
+    return set_error(ZNTT_ERR_INVALID_ARGUMENT, "the node array must be 16-byte aligned");
+  RowColumns C;
+  for (uint32_t c = 0; c < 256; c++) C.col[c] = nullptr;
+  for (uint32_t c = 0; c < num_columns; c++) {
+    if (!d_columns[c]) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null column");
+    C.col[c] = d_columns[c];
+  }
+  for (size_t q = 0; q < num_queries; q++)
+    if (positions[q] >> log_n) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "a row outside the commitment");
+  Context& c = ctx();
+  if (c.device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+  const size_t path_bytes = num_queries * log_n * 32, value_bytes = num_queries * num_columns * nb;
+  const size_t vo = (path_bytes + 15) / 16 * 16, po = (vo + value_bytes + 15) / 16 * 16;
+  const size_t bytes = po + num_queries * 8;
+  void* stage = nullptr;
+  rc = pool_get(bytes, &stage);
+  if (rc) return rc;
+  uint8_t* s = static_cast<uint8_t*>(stage);
+  uint64_t* d_pos = reinterpret_cast<uint64_t*>(s + po);
+  cudaError_t ce = cudaMemcpyAsync(d_pos, positions, num_queries * 8, cudaMemcpyHostToDevice, st);
+  if (ce == cudaSuccess) {
+    const uint32_t nq = (uint32_t)num_queries;
+    const int grid = (int)((nq + 127) / 128);
+    const uint4* nodes = reinterpret_cast<const uint4*>(d_nodes);
+    uint32_t* vals = reinterpret_cast<uint32_t*>(s + vo);
+    uint4* paths = reinterpret_cast<uint4*>(s);
+    switch (field) {
+      case kBn254Fr:
+        open_rows_kernel<kBn254Fr><<<grid, 128, 0, st>>>(C, num_columns, log_n, nodes, d_pos, nq, vals, paths);
+        break;
+      case kBls12381Fr:
+        open_rows_kernel<kBls12381Fr><<<grid, 128, 0, st>>>(C, num_columns, log_n, nodes, d_pos, nq, vals, paths);
+        break;
+      case kGoldilocksField:
+        open_rows_kernel<kGoldilocksField><<<grid, 128, 0, st>>>(C, num_columns, log_n, nodes, d_pos, nq, vals, paths);
+        break;
+      default:
+        open_rows_kernel<kBabyBearField><<<grid, 128, 0, st>>>(C, num_columns, log_n, nodes, d_pos, nq, vals, paths);
+    }
+    ce = cudaGetLastError();
+  }
+  if (ce == cudaSuccess && path_bytes) ce = cudaMemcpyAsync(paths_out, s, path_bytes, cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(values_out, s + vo, value_bytes, cudaMemcpyDeviceToHost, st);
+  cudaError_t ce2 = cudaStreamSynchronize(st);  // the staging buffer returns to the pool
+  if (ce == cudaSuccess) ce = ce2;
+  if (ce2 == cudaSuccess) pool_put(stage, bytes);
+  if (ce != cudaSuccess) return cuda_fail(ce, "row openings");
+  return ZNTT_OK;
+}
