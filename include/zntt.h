@@ -38,7 +38,8 @@ enum zntt_status {
   ZNTT_ERR_INVALID_LENGTH = 4,     /* error.InvalidLength: bitReverse len 0 / not 2^k (root.zig:43) */
   ZNTT_ERR_OUT_OF_MEMORY = 5,      /* error.OutOfMemory, or the vector does not fit on the device */
   ZNTT_ERR_ORDER_TOO_LARGE = 6,    /* error.OrderTooLarge: log_n > two-adicity (roots.zig:150) */
-  ZNTT_ERR_UNSUPPORTED_FIELD = 7,  /* a field id other than the two below */
+  ZNTT_ERR_UNSUPPORTED_FIELD = 7,  /* a field id other than the four below, or a small field
+                                      where only the 256-bit ones are served */
   ZNTT_ERR_DEVICE = 8,             /* a CUDA call failed; see zntt_last_error() */
   ZNTT_ERR_TIMEOUT = 9,            /* a bounded device wait gave up */
   ZNTT_ERR_INVALID_ARGUMENT = 10,  /* null pointer, bad handle, unknown mode */
@@ -56,11 +57,12 @@ enum zntt_field {
    * reference's own transform known-answer tests (libs/ntt/src/root.zig:437-447).  An element
    * is SmallField's canonical value, ONE uint64_t (8 bytes), not four Montgomery limbs; roots
    * and other scalars still pass as uint64_t[4] with the value in [0] and zeros after.  These
-   * fields serve the seven zig-ntt entry points, zntt_field_info / zntt_primitive_root and the
-   * device API (zntt_twiddles_acquire / _release, zntt_ntt_device); bitReverse of 8-byte
-   * elements is zntt_bit_reverse_small.  Batches, coset extensions, polynomial products, the
-   * server, the pipelined host API and the allocation-free entry point take the 256-bit fields
-   * only and reject a small-field table with ZNTT_ERR_UNSUPPORTED_FIELD. */
+   * fields serve the seven zig-ntt entry points, zntt_field_info / zntt_primitive_root, the
+   * device API (zntt_twiddles_acquire / _release, zntt_ntt_device), zntt_coset_lde_device, and
+   * the FRI and Merkle entry points; bitReverse of 8-byte elements is zntt_bit_reverse_small.
+   * Batches, polynomial products, the server, the pipelined host API and the allocation-free
+   * entry point take the 256-bit fields only and reject a small-field table with
+   * ZNTT_ERR_UNSUPPORTED_FIELD. */
   ZNTT_FIELD_GOLDILOCKS = 2,    /* p = 2^64 - 2^32 + 1, two-adicity 32 */
   ZNTT_FIELD_BABYBEAR = 3       /* p = 15 * 2^27 + 1, two-adicity 27 */
 };
