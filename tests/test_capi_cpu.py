@@ -143,6 +143,13 @@ def test_fri_prover_loop_arguments_before_any_device_work(zntt):
         zntt.fri_fold_commit(F, 1 << 20, 6, [2**64 - 1] * 4, 1 << 24, 1 << 28)  # alpha >= p
     with pytest.raises(zntt.UnsupportedField):
         zntt.fri_fold_commit(zntt.Field(9, "bogus", 7, 1), 1 << 20, 6, [0, 0, 0, 0], 1 << 24, 1 << 28)
+    cols = (ctypes.c_void_p * 1)(1 << 20)
+    for count in (0, 33, 1 << 27):  # no column, a row beyond one chunk, a byte size that wraps 32 bits
+        with pytest.raises(zntt.InvalidArgument):
+            zntt._check(zntt.lib().zntt_merkle_commit_rows(F.id, cols, count, 4, 1 << 28, None, None))
+        with pytest.raises(zntt.InvalidArgument):
+            zntt._check(zntt.lib().zntt_merkle_open_rows(F.id, cols, count, 4, 1 << 28,
+                                                         (ctypes.c_uint64 * 1)(0), 1, b"x" * 64, b"x" * 64, None))
 
 
 def test_small_fields_host_side(zntt, oracle):

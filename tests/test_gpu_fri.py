@@ -6,6 +6,7 @@ table; at full size the fold identity fold(evals of p) = evals of p_even + alpha
 every opened path authenticates against its round's root.  Needs a B200."""
 from __future__ import annotations
 
+import ctypes
 import os
 
 import numpy as np
@@ -478,6 +479,8 @@ def test_row_commitment_argument_checks(z):
         z.merkle_commit_rows(F, [col] * 33, 4, nodes)
     with pytest.raises(z.InvalidArgument):
         z.merkle_commit_rows(F, [col, 0], 4, nodes)
+    with pytest.raises(z.InvalidArgument):  # a column count whose byte size wraps 32 bits
+        z._check(z.lib().zntt_merkle_commit_rows(F.id, (ctypes.c_void_p * 1)(col), 1 << 27, 4, nodes, None, None))
     with pytest.raises(z.InvalidArgument):
         z.merkle_commit_rows(F, [], 4, nodes)
     with pytest.raises(z.InvalidArgument):  # the nodes overlap the column

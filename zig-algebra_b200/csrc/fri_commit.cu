@@ -633,7 +633,7 @@ extern "C" int zntt_merkle_commit_rows(int field, const uint64_t* const* d_colum
     return set_error(ZNTT_ERR_UNSUPPORTED_FIELD, "unsupported field");
   if (!d_columns || !d_nodes) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
   const uint32_t nb = small ? (field == kGoldilocksField ? 8u : 4u) : 32u;
-  if (num_columns == 0 || num_columns * nb > 1024)
+  if (num_columns == 0 || num_columns > 1024 / nb)  // a row of at most 1024 bytes (no overflow)
     return set_error(ZNTT_ERR_INVALID_ARGUMENT, "rows of 1 .. 1024 bytes (one BLAKE3 chunk)");
   if (log_n > 30) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "at most 2^30 rows");
   if (reinterpret_cast<uintptr_t>(d_nodes) % 16)

@@ -258,7 +258,7 @@ extern "C" int zntt_merkle_open_rows(int field, const uint64_t* const* d_columns
   const uint32_t nb = element_bytes(field);
   if (!d_columns || !d_nodes || !positions || !values_out || (!paths_out && log_n > 0))
     return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
-  if (num_columns == 0 || num_columns * nb > 1024)
+  if (num_columns == 0 || num_columns > 1024 / nb)  // a row of at most 1024 bytes (no overflow)
     return set_error(ZNTT_ERR_INVALID_ARGUMENT, "rows of 1 .. 1024 bytes (one BLAKE3 chunk)");
   if (log_n > 30) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "at most 2^30 rows");
   if (num_queries == 0 || num_queries > (1u << 20)) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "1 .. 2^20 queries");
