@@ -712,7 +712,7 @@ def cpu_fri_sample(fid_name, log_sample=20):
     commitment (hashPair + BLAKE3 Merkle tree) on one 2^log_sample layer, all host cores."""
     workers = min(os.cpu_count() or 1, 64)
     O, _ = cpu_oracle(native=True)
-    fid = {"bn254_fr": O.BN254_FR, "goldilocks": O.GOLDILOCKS}[fid_name]
+    fid = {"bn254_fr": O.BN254_FR, "goldilocks": O.GOLDILOCKS, "babybear": O.BABYBEAR}[fid_name]
     n = 1 << log_sample
     layer = O.random_elements(fid, 5, n)
     alpha = O.random_elements(fid, 6, 1)[0]
@@ -739,8 +739,8 @@ def run_fri_config(z, torch, stream, steps, warmup, log_n=24, cpu_sample=True):
     out = {"workload": f"FRI fold of a 2^{log_n}-evaluation layer, the chain 2^{log_n} -> 2^10, and the "
                        f"layer's BLAKE3 Merkle commitment",
            "fields": {}}
-    for F in (z.BN254_FR, z.GOLDILOCKS):
-        ew = 8 * F.limbs  # bytes per element
+    for F in (z.BN254_FR, z.GOLDILOCKS, z.BABYBEAR):
+        ew = 8 * F.limbs  # bytes per element in device memory
         n = 1 << log_n
         layer = torch.empty(n * F.limbs, dtype=torch.int64, device="cuda")
         if F.limbs == 4:
@@ -774,7 +774,7 @@ def run_fri_config(z, torch, stream, steps, warmup, log_n=24, cpu_sample=True):
         # The openings through the C ABI into preallocated host buffers (the Python wrapper's
         # unpacking into per-query lists is not library time).
         import ctypes
-        nb = 32 if F.limbs == 4 else 8
+        nb = z._num_bytes(F)  # toBytes length
         per_query = sum(log_n - r - 1 for r in range(rounds))
         q_vals = ctypes.create_string_buffer(64 * rounds * 2 * nb)
         q_paths = ctypes.create_string_buffer(64 * per_query * 32)
@@ -810,7 +810,7 @@ def run_fri_config(z, torch, stream, steps, warmup, log_n=24, cpu_sample=True):
         for _ in range(warmup):
             rcommit()
         ms_rows = time_region(torch, stream, rcommit, steps) / steps
-        rows_compressions = rows * -(-ncol * ew // 64) + rows - 1
+        rows_compressions = rows * -(-ncol * z._num_bytes(F) // 64) + rows - 1
         del cols, rnodes
         layer_copy = layer.clone()  # the commit phase folds into bufs; layer 0 is only read
         for _ in range(2):
@@ -954,7 +954,7 @@ def run_single_config(args):
                                cpu_sample=not args.no_cpu_baseline)
             r["value"] = r["fields"]["bn254_fr"]["fold_value"]
             r["unit"] = "output elements/s"
-            metric = "BN254-Fr FRI fold output elems/s (2^24 -> 2^23; Goldilocks beside it)"
+            metric = "BN254-Fr FRI fold output elems/s (2^24 -> 2^23; Goldilocks and BabyBear beside it)"
         elif args.workload == "poly":
             r = run_poly_config(z, torch, stream, steps=args.steps, warmup=args.warmup,
                                 cpu_sample=not args.no_cpu_baseline)
