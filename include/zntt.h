@@ -60,9 +60,9 @@ enum zntt_field {
    * fields serve the seven zig-ntt entry points, zntt_field_info / zntt_primitive_root, the
    * device API (zntt_twiddles_acquire / _release, zntt_ntt_device), zntt_coset_lde_device, and
    * the FRI and Merkle entry points; bitReverse of 8-byte elements is zntt_bit_reverse_small.
-   * Batches, polynomial products, the server, the pipelined host API and the allocation-free
-   * entry point take the 256-bit fields only and reject a small-field table with
-   * ZNTT_ERR_UNSUPPORTED_FIELD. */
+   * zntt_poly_mul also serves them.  Batches, zntt_poly_mul_device, the server, the
+   * pipelined host API and the allocation-free entry point take the 256-bit fields only and
+   * reject a small-field table with ZNTT_ERR_UNSUPPORTED_FIELD. */
   ZNTT_FIELD_GOLDILOCKS = 2,    /* p = 2^64 - 2^32 + 1, two-adicity 32 */
   ZNTT_FIELD_BABYBEAR = 3       /* p = 15 * 2^27 + 1, two-adicity 27 */
 };
@@ -223,7 +223,10 @@ int zntt_poly_mul_device(const zntt_twiddles* tw, const uint64_t* d_a, size_t le
  * polynomial; a product degree above max_degree is ZNTT_ERR_DEGREE_TOO_LARGE
  * (poly.zig:198-200).  On success out[0 .. max_degree] holds the product's
  * coefficients followed by zeros (the reference's fixed coeffs array) and
- * *out_degree its degree, -1 for the zero polynomial.  Synchronous. */
+ * *out_degree its degree, -1 for the zero polynomial.  Synchronous.  All four
+ * fields: coefficients are four Montgomery limbs each for the 256-bit fields and one
+ * canonical uint64_t each (below p, else ZNTT_ERR_INVALID_ARGUMENT) for Goldilocks and
+ * BabyBear. */
 int zntt_poly_mul(int field, const uint64_t* a, size_t a_len, const uint64_t* b, size_t b_len, size_t max_degree,
                   uint64_t* out, int64_t* out_degree);
 

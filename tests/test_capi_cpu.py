@@ -152,6 +152,23 @@ def test_fri_prover_loop_arguments_before_any_device_work(zntt):
                                                          (ctypes.c_uint64 * 1)(0), 1, b"x" * 64, b"x" * 64, None))
 
 
+def test_small_field_poly_mul_contract_before_any_device_work(zntt):
+    """Polynomial.mul's results that need no transform, for Goldilocks and BabyBear (one
+    canonical u64 per coefficient): the zero polynomial, both DegreeTooLarge cases, and a
+    non-canonical coefficient refused."""
+    for F in (zntt.GOLDILOCKS, zntt.BABYBEAR):
+        b = np.array([3, 1, 4], dtype=np.uint64)
+        out, deg = zntt.poly_mul(F, np.zeros(3, dtype=np.uint64), b, 10)
+        assert deg == -1 and not out.any() and out.shape == (11,)
+        a = np.array([2, 7, 1, 8, 2, 8], dtype=np.uint64)
+        with pytest.raises(zntt.DegreeTooLarge):
+            zntt.poly_mul(F, a, b, 6)  # product degree 7 > 6
+        with pytest.raises(zntt.DegreeTooLarge):
+            zntt.poly_mul(F, a, b[:1], 4)  # six coefficients do not fit max_degree 4
+        with pytest.raises(zntt.InvalidArgument):
+            zntt.poly_mul(F, np.array([F.modulus], dtype=np.uint64), b, 10)
+
+
 def test_small_fields_host_side(zntt, oracle):
     """Goldilocks and BabyBear: field info, primitive roots as zig-field derives them (the
     roots of the reference's KAT, libs/ntt/src/root.zig:437-447, and the oracle's at every

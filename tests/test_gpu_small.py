@@ -221,3 +221,20 @@ def test_small_tables_are_refused_by_256_bit_entry_points(z):
         with pytest.raises((z.UnsupportedField, z.InvalidArgument)):
             z.Batch(z.BN254_FR, [{"kind": z.JOB_NTT, "tw": t, "mode": z.FORWARD, "src": buf.data_ptr(),
                                   "dst": buf[1024:].data_ptr()}])
+
+
+@pytest.mark.parametrize("la,lb", [(1, 1), (5, 3), (300, 200), (1 << 12, 1 << 12), ((1 << 15) + 3, 1 << 14)])
+def test_poly_mul_matches_oracle(z, la, lb):
+    """zntt_poly_mul over Goldilocks and BabyBear against the oracle's schoolbook product
+    (Polynomial.mul, libs/poly/src/poly.zig:197-212): coefficients, degree and the zero tail."""
+    for F, fid in _fields(z):
+        a = _random(fid, 2000 + la, la)
+        b = _random(fid, 3000 + lb, lb)
+        a[-1] = a[-1] or 1  # keep the leading coefficients non-zero
+        b[-1] = b[-1] or 1
+        max_degree = la + lb + 5
+        got, deg = z.poly_mul(F, a, b, max_degree)
+        workers = WORKERS if la * lb > 1 << 20 else 1
+        st, want, wdeg = O.poly_mul(fid, _slots(fid, a), _slots(fid, b), max_degree, workers=workers)
+        assert st == O.OK and deg == wdeg == la + lb - 2
+        np.testing.assert_array_equal(got, _canon(fid, want), err_msg=f"{F.name} {la} x {lb}")

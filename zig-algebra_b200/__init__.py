@@ -573,12 +573,14 @@ def poly_mul_device(tw: DeviceTwiddles, d_a: int, len_a: int, d_b: int, len_b: i
 def poly_mul(F: Field, a: np.ndarray, b: np.ndarray, max_degree: int):
     """Polynomial(F, max_degree).fromCoeffs(a).mul(fromCoeffs(b)) (libs/poly/src/poly.zig:76-84,
     197-212) on the device: returns (coefficients, an (max_degree + 1, 4) uint64 array of
-    Montgomery limbs, zero beyond the degree; degree, -1 for the zero polynomial).  Raises
-    DegreeTooLarge as the reference does."""
+    Montgomery limbs -- (max_degree + 1,) canonical values for Goldilocks and BabyBear -- zero
+    beyond the degree; degree, -1 for the zero polynomial).  Raises DegreeTooLarge as the
+    reference does."""
     _ensure_init()
-    a = np.ascontiguousarray(np.asarray(a, dtype=np.uint64).reshape(-1, 4))
-    b = np.ascontiguousarray(np.asarray(b, dtype=np.uint64).reshape(-1, 4))
-    out = np.zeros((max_degree + 1, 4), dtype=np.uint64)
+    shape = (-1, 4) if F.limbs == 4 else (-1,)  # small fields: one canonical u64 per coefficient
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.uint64).reshape(shape))
+    b = np.ascontiguousarray(np.asarray(b, dtype=np.uint64).reshape(shape))
+    out = np.zeros((max_degree + 1, 4) if F.limbs == 4 else (max_degree + 1,), dtype=np.uint64)
     deg = ctypes.c_int64(0)
     pa = a.ctypes.data_as(_U64P) if len(a) else None
     pb = b.ctypes.data_as(_U64P) if len(b) else None

@@ -102,6 +102,7 @@ int zntt_poly_mul_device(const zntt_twiddles* tw, const uint64_t* d_a, size_t le
 int zntt_poly_mul(int field, const uint64_t* a, size_t a_len, const uint64_t* b, size_t b_len, size_t max_degree,
                   uint64_t* out, int64_t* out_degree) {
   clear_error();
+  if (is_small_field(field)) return small_poly_mul(field, a, a_len, b, b_len, max_degree, out, out_degree);
   if (field != kBn254Fr && field != kBls12381Fr) return set_error(ZNTT_ERR_UNSUPPORTED_FIELD, "unsupported field");
   if ((a_len && !a) || (b_len && !b) || !out || !out_degree) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
   if (max_degree >= ((size_t)1 << 58)) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "max_degree out of range");

@@ -248,6 +248,15 @@ __global__ void small_coset_scale_kernel(const uint64_t* __restrict__ pw, uint64
   }
 }
 
+// out[i] = a[i] * b[i] for canonical values: mul(a, R^2) is a in twiddle form
+// (a R), whose product with the canonical b is canonical.
+template <class SF>
+__global__ void small_pointwise_kernel(const uint64_t* a, const uint64_t* __restrict__ b, uint64_t* out,
+                                       uint64_t count, uint64_t r2) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = SF::mul(SF::mul(a[i], r2), b[i]);
+}
+
 // One FRI fold round (libs/fri/src/root.zig:396-403) on canonical values;
 // half_inv, alpha and the table g^-j / 2 are in twiddle form.
 template <class SF>
@@ -1024,6 +1033,96 @@ int small_coset_lde(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, con
   if (rc) return rc;
   if (ce == cudaSuccess) ce = ce2;
   if (ce != cudaSuccess) return cuda_fail(ce, "coset extension");
+  return ZNTT_OK;
+}
+
+}  // namespace zntt
+
+namespace zntt {
+
+// Polynomial(F, max_degree).mul (libs/poly/src/poly.zig:197-212) for a small
+// field, host coefficients one canonical u64 each: the same contract as the
+// 256-bit path (fromCoeffs' length check, the zero polynomial, DegreeTooLarge,
+// zero fill beyond the degree), computed as forward(a), forward(b), their
+// pointwise product, and the inverse with 1/n over n = 2^L >= deg a + deg b + 1.
+int small_poly_mul(int field, const uint64_t* a, size_t a_len, const uint64_t* b, size_t b_len, size_t max_degree,
+                   uint64_t* out, int64_t* out_degree) {
+  const SmallHost& H = small_host(field);
+  if ((a_len && !a) || (b_len && !b) || !out || !out_degree) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
+  if (max_degree >= ((size_t)1 << 58)) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "max_degree out of range");
+  if (a_len > max_degree + 1 || b_len > max_degree + 1)
+    return set_error(ZNTT_ERR_DEGREE_TOO_LARGE, "a factor has more than max_degree + 1 coefficients");
+  auto degree_of = [](const uint64_t* c, size_t len) {
+    int64_t d = (int64_t)len - 1;
+    while (d >= 0 && c[d] == 0) d--;
+    return d;
+  };
+  for (size_t i = 0; i < a_len; i++)
+    if (a[i] >= H.p) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "a coefficient is not canonical");
+  for (size_t i = 0; i < b_len; i++)
+    if (b[i] >= H.p) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "a coefficient is not canonical");
+  const int64_t da = degree_of(a, a_len), db = degree_of(b, b_len);
+  if (da < 0 || db < 0) {  // a zero factor: the zero polynomial (poly.zig:198)
+    std::memset(out, 0, (max_degree + 1) * 8);
+    *out_degree = -1;
+    return ZNTT_OK;
+  }
+  const int64_t d = da + db;
+  if ((uint64_t)d > max_degree)
+    return set_error(ZNTT_ERR_DEGREE_TOO_LARGE, "the product's degree exceeds max_degree (Polynomial.mul)");
+  uint32_t L = 0;
+  while ((1ull << L) < (uint64_t)d + 1) L++;
+  if (L > H.two_adicity) return set_error(ZNTT_ERR_ORDER_TOO_LARGE, "the product needs a transform beyond the two-adicity");
+  Context& c = ctx();
+  if (c.device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  uint64_t root[4];
+  int rc = small_primitive_root(field, L, root);
+  if (rc) return rc;
+  zntt_twiddles* tw = nullptr;
+  rc = small_twiddles_acquire(field, L, root, &tw);
+  if (rc) return rc;
+  const SmallTable* t = reinterpret_cast<const SmallTable*>(tw);
+  const uint64_t n = 1ull << L;
+  const size_t la = (size_t)da + 1, lb = (size_t)db + 1, lo = (size_t)d + 1;
+  void* dev[3] = {nullptr, nullptr, nullptr};  // A, B (n each), scratch (n)
+  for (int i = 0; i < 3 && !rc; i++) rc = pool_get(n * 8, &dev[i]);
+  cudaStream_t st = c.stream;
+  uint64_t* A = static_cast<uint64_t*>(dev[0]);
+  uint64_t* B = static_cast<uint64_t*>(dev[1]);
+  uint64_t* S = static_cast<uint64_t*>(dev[2]);
+  cudaError_t ce = cudaSuccess;
+  if (!rc) {
+    ce = cudaMemcpyAsync(A, a, la * 8, cudaMemcpyHostToDevice, st);
+    if (ce == cudaSuccess && n > la) ce = cudaMemsetAsync(A + la, 0, (n - la) * 8, st);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(B, b, lb * 8, cudaMemcpyHostToDevice, st);
+    if (ce == cudaSuccess && n > lb) ce = cudaMemsetAsync(B + lb, 0, (n - lb) * 8, st);
+    if (ce != cudaSuccess) rc = cuda_fail(ce, "polynomial upload");
+  }
+  if (!rc) rc = small_run(t, A, A, S, false, false, 0, st);
+  if (!rc) rc = small_run(t, B, B, S, false, false, 0, st);
+  if (!rc) {
+    const uint64_t r2 = H.mul(H.r, H.r);
+    if (field == kGoldilocksField)
+      small_pointwise_kernel<Goldilocks><<<grid_for(n), 256, 0, st>>>(A, B, A, n, r2);
+    else
+      small_pointwise_kernel<BabyBear><<<grid_for(n), 256, 0, st>>>(A, B, A, n, r2);
+    ce = cudaGetLastError();
+    if (ce != cudaSuccess) rc = cuda_fail(ce, "pointwise product");
+  }
+  if (!rc) rc = small_run(t, A, B, S, true, true, n_inverse_tw(H, L), st);  // coefficients into B
+  if (!rc) {
+    ce = cudaMemcpyAsync(out, B, lo * 8, cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) rc = cuda_fail(ce, "polynomial download");
+  }
+  if (rc) cudaStreamSynchronize(st);  // no copy or kernel may still use a pooled buffer
+  for (int i = 0; i < 3; i++)
+    if (dev[i]) pool_put(dev[i], n * 8);
+  small_twiddles_release(tw);
+  if (rc) return rc;
+  std::memset(out + lo, 0, (max_degree + 1 - lo) * 8);
+  *out_degree = degree_of(out, lo);
   return ZNTT_OK;
 }
 
