@@ -700,6 +700,29 @@ def run_small_config(z, torch, stream, steps, warmup, log_n=24, cpu_sample=True)
             r["lde_ms"] = time_region(torch, stream, lde, steps) / steps
         r["lde_note"] = (f"coset extension 2^{lin} -> 2^{log_n} (zntt_coset_lde_device; the call waits for "
                          f"its stream)")
+        # A STARK trace commitment: 64 columns of 2^18 rows extended to 2^20 (zntt_coset_lde_columns),
+        # then the 2^20 rows committed (zntt_merkle_commit_rows).
+        m, t_in, t_out = 64, 18, 20
+        tcols = [torch.from_numpy(np.random.default_rng(300 + k).integers(0, F.modulus, 1 << t_in, dtype=np.uint64)
+                                  .view(np.int64)).cuda() for k in range(m)]
+        touts = [torch.empty(1 << t_out, dtype=torch.int64, device="cuda") for _ in range(m)]
+        tnodes = torch.empty((2 << t_out) * 4, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        with z.DeviceTwiddles(F, t_in, z.primitiveRootOfUnity(F, t_in)) as ti, \
+                z.DeviceTwiddles(F, t_out, z.primitiveRootOfUnity(F, t_out)) as to:
+            shift = np.array([7, 0, 0, 0], dtype=np.uint64)
+            ins, outs_p = [c_.data_ptr() for c_ in tcols], [o.data_ptr() for o in touts]
+            ext = lambda: z.coset_lde_columns(ti, to, shift, ins, outs_p, stream=sptr)  # noqa: E731
+            com = lambda: z.merkle_commit_rows(F, outs_p, t_out, tnodes.data_ptr(), stream=sptr)  # noqa: E731
+            for _ in range(2):
+                ext()
+                com()
+            k_t = max(steps // 4, 2)
+            r["trace"] = {"columns": m, "rows_in": 1 << t_in, "rows_out": 1 << t_out,
+                          "extend_ms": time_region(torch, stream, ext, k_t) / k_t,
+                          "commit_ms": time_region(torch, stream, com, k_t) / k_t,
+                          "note": "a STARK trace commitment: zntt_coset_lde_columns then zntt_merkle_commit_rows"}
+        del tcols, touts, tnodes
         if cpu_sample:
             r["cpu_baseline"] = cpu_small_sample(F, xs, log_n)
         out["fields"][F.name] = r

@@ -238,3 +238,30 @@ def test_poly_mul_matches_oracle(z, la, lb):
         st, want, wdeg = O.poly_mul(fid, _slots(fid, a), _slots(fid, b), max_degree, workers=workers)
         assert st == O.OK and deg == wdeg == la + lb - 2
         np.testing.assert_array_equal(got, _canon(fid, want), err_msg=f"{F.name} {la} x {lb}")
+
+
+def test_coset_lde_columns_equal_single_extensions(z):
+    """zntt_coset_lde_columns (the columns back to back on one stream) equals one
+    zntt_coset_lde_device call per column, for the small fields and BN254-Fr."""
+    torch = pytest.importorskip("torch")
+    cases = [(z.GOLDILOCKS, O.GOLDILOCKS, 5), (z.BABYBEAR, O.BABYBEAR, 3), (z.BN254_FR, O.BN254_FR, 2)]
+    for F, fid, m in cases:
+        log_in, log_out = 10, 12
+        if F.limbs == 4:
+            cols = [torch.from_numpy(O.random_elements(fid, 50 + k, 1 << log_in).view(np.int64).reshape(-1).copy()).cuda()
+                    for k in range(m)]
+            shift = z.to_montgomery(F, 5)
+        else:
+            cols = [torch.from_numpy(_random(fid, 50 + k, 1 << log_in).view(np.int64).copy()).cuda() for k in range(m)]
+            shift = np.array([7, 0, 0, 0], dtype=np.uint64)
+        outs = [torch.empty((1 << log_out) * F.limbs, dtype=torch.int64, device="cuda") for _ in range(m)]
+        wants = [torch.empty_like(o) for o in outs]
+        torch.cuda.synchronize()
+        with z.DeviceTwiddles(F, log_in, z.primitiveRootOfUnity(F, log_in)) as ti, \
+                z.DeviceTwiddles(F, log_out, z.primitiveRootOfUnity(F, log_out)) as to:
+            z.coset_lde_columns(ti, to, shift, [c.data_ptr() for c in cols], [o.data_ptr() for o in outs])
+            for c, w in zip(cols, wants):
+                z.coset_lde_device(ti, to, shift, c.data_ptr(), w.data_ptr())
+        torch.cuda.synchronize()
+        for k, (o, w) in enumerate(zip(outs, wants)):
+            assert torch.equal(o, w), (F.name, k)

@@ -215,6 +215,8 @@ def lib():
                                       ctypes.POINTER(i), ctypes.POINTER(i)]
         L.zntt_batch_destroy.argtypes = [vp]
         L.zntt_coset_lde_device.argtypes = [vp, vp, _U64P, vp, vp, vp]
+        L.zntt_coset_lde_columns.argtypes = [vp, vp, _U64P, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_uint32,
+                                             vp]
         L.zntt_poly_mul_device.argtypes = [vp, vp, sz, vp, sz, vp, vp]
         L.zntt_fri_domain_fill.argtypes = [i, ctypes.c_uint32, vp, vp]
         L.zntt_fri_fold_device.argtypes = [i, vp, ctypes.c_uint32, _U64P, vp, ctypes.c_uint32, vp]
@@ -560,6 +562,16 @@ def coset_lde_device(tw_in: DeviceTwiddles, tw_out: DeviceTwiddles, shift, d_eva
                      stream: int = 0) -> None:
     """One coset low-degree extension with plain per-pass launches."""
     _check(lib().zntt_coset_lde_device(tw_in.handle, tw_out.handle, _root(shift), d_evals, d_out, stream or None))
+
+
+def coset_lde_columns(tw_in: DeviceTwiddles, tw_out: DeviceTwiddles, shift, d_evals, d_outs,
+                      stream: int = 0) -> None:
+    """The coset extension of several columns (zntt_coset_lde_columns): column k from d_evals[k]
+    into d_outs[k]."""
+    m = len(d_evals)
+    ev = (ctypes.c_void_p * max(m, 1))(*d_evals)
+    out = (ctypes.c_void_p * max(len(d_outs), 1))(*d_outs)
+    _check(lib().zntt_coset_lde_columns(tw_in.handle, tw_out.handle, _root(shift), ev, out, m, stream or None))
 
 
 def poly_mul_device(tw: DeviceTwiddles, d_a: int, len_a: int, d_b: int, len_b: int, d_out: int,

@@ -459,6 +459,26 @@ int zntt_coset_lde_device(const zntt_twiddles* tw_in, const zntt_twiddles* tw_ou
   return ZNTT_OK;
 }
 
+int zntt_coset_lde_columns(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t shift[4],
+                           const uint64_t* const* d_evals, uint64_t* const* d_out, uint32_t num_columns,
+                           void* stream) {
+  clear_error();
+  if (!tw_in || !tw_out || !shift || !d_evals || !d_out) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
+  if (num_columns == 0) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "no columns");
+  Context& c = ctx();
+  if (c.device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
+  if (is_small_table(tw_in) != is_small_table(tw_out))
+    return set_error(ZNTT_ERR_INVALID_ARGUMENT, "tables of different fields");
+  if (is_small_table(tw_in)) return small_coset_lde_many(tw_in, tw_out, shift, d_evals, d_out, num_columns, stream);
+  // The 256-bit fields: one extension per column (a batch of ZNTT_JOB_COSET_LDE jobs
+  // runs them in one persistent launch instead).
+  for (uint32_t k = 0; k < num_columns; k++) {
+    const int rc = zntt_coset_lde_device(tw_in, tw_out, shift, d_evals[k], d_out[k], stream);
+    if (rc) return rc;
+  }
+  return ZNTT_OK;
+}
+
 // ---- autotuner ---------------------------------------------------------------------
 
 int zntt_autotune(int field, uint32_t log_n_min, uint32_t log_n_max) {

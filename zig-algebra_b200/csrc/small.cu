@@ -976,8 +976,8 @@ namespace zntt {
 // inverse transform of the 2^log_in evaluations into the head of d_out (with
 // 1/n), coefficient i times shift^i, the tail zeroed, and the forward
 // transform of d_out in place.
-int small_coset_lde(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t* shift,
-                    const uint64_t* d_evals, uint64_t* d_out, void* stream) {
+int small_coset_lde_many(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t* shift,
+                         const uint64_t* const* d_evals, uint64_t* const* d_out, uint32_t m, void* stream) {
   const SmallTable* ti = reinterpret_cast<const SmallTable*>(tw_in);
   const SmallTable* to = reinterpret_cast<const SmallTable*>(tw_out);
   if (ti->field != to->field) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "tables of different fields");
@@ -987,9 +987,12 @@ int small_coset_lde(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, con
   if (shift[1] || shift[2] || shift[3] || shift[0] >= H.p || shift[0] == 0)
     return set_error(ZNTT_ERR_INVALID_ARGUMENT, "the shift must be a nonzero canonical element in word 0");
   const uint64_t n_in = 1ull << ti->log_n, n_out = 1ull << to->log_n;
-  const char* eo = reinterpret_cast<const char*>(d_evals);
-  const char* oo = reinterpret_cast<const char*>(d_out);
-  if (oo < eo + n_in * 8 && eo < oo + n_out * 8) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "extension in place");
+  for (uint32_t k = 0; k < m; k++) {
+    if (!d_evals[k] || !d_out[k]) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null column");
+    const char* eo = reinterpret_cast<const char*>(d_evals[k]);
+    const char* oo = reinterpret_cast<const char*>(d_out[k]);
+    if (oo < eo + n_in * 8 && eo < oo + n_out * 8) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "extension in place");
+  }
   Context& c = ctx();
   std::lock_guard<std::recursive_mutex> lock(c.mu);
   cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
@@ -1013,18 +1016,20 @@ int small_coset_lde(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, con
     pool_put(d_pw, pw.size() * 8);
     return rc;
   }
+  // One stream: the columns run one after another and share the power tables and
+  // the forward transform's scratch.
   cudaError_t ce = cudaMemcpyAsync(d_pw, pw.data(), pw.size() * 8, cudaMemcpyHostToDevice, st);
-  if (ce == cudaSuccess) {
-    rc = small_run(ti, d_evals, d_out, nullptr, true, true, n_inverse_tw(H, ti->log_n), st);  // out of place
-    if (rc == ZNTT_OK) {
-      if (ti->field == kGoldilocksField)
-        small_coset_scale_kernel<Goldilocks><<<grid_for(n_in), 256, 0, st>>>((const uint64_t*)d_pw, d_out, n_in);
-      else
-        small_coset_scale_kernel<BabyBear><<<grid_for(n_in), 256, 0, st>>>((const uint64_t*)d_pw, d_out, n_in);
-      ce = cudaGetLastError();
-      if (ce == cudaSuccess && n_out > n_in) ce = cudaMemsetAsync(d_out + n_in, 0, (n_out - n_in) * 8, st);
-      if (ce == cudaSuccess) rc = small_run(to, d_out, d_out, (uint64_t*)scratch, false, false, 0, st);
-    }
+  for (uint32_t k = 0; k < m && ce == cudaSuccess && rc == ZNTT_OK; k++) {
+    uint64_t* out = d_out[k];
+    rc = small_run(ti, d_evals[k], out, nullptr, true, true, n_inverse_tw(H, ti->log_n), st);  // out of place
+    if (rc) break;
+    if (ti->field == kGoldilocksField)
+      small_coset_scale_kernel<Goldilocks><<<grid_for(n_in), 256, 0, st>>>((const uint64_t*)d_pw, out, n_in);
+    else
+      small_coset_scale_kernel<BabyBear><<<grid_for(n_in), 256, 0, st>>>((const uint64_t*)d_pw, out, n_in);
+    ce = cudaGetLastError();
+    if (ce == cudaSuccess && n_out > n_in) ce = cudaMemsetAsync(out + n_in, 0, (n_out - n_in) * 8, st);
+    if (ce == cudaSuccess) rc = small_run(to, out, out, (uint64_t*)scratch, false, false, 0, st);
   }
   // The power tables and the scratch return to the pool after the stream is done.
   cudaError_t ce2 = cudaStreamSynchronize(st);
@@ -1034,6 +1039,11 @@ int small_coset_lde(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, con
   if (ce == cudaSuccess) ce = ce2;
   if (ce != cudaSuccess) return cuda_fail(ce, "coset extension");
   return ZNTT_OK;
+}
+
+int small_coset_lde(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t* shift,
+                    const uint64_t* d_evals, uint64_t* d_out, void* stream) {
+  return small_coset_lde_many(tw_in, tw_out, shift, &d_evals, &d_out, 1, stream);
 }
 
 }  // namespace zntt
