@@ -201,9 +201,10 @@ int zntt_batch_destroy(zntt_batch* b);
 int zntt_coset_lde_device(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t shift[4],
                           const uint64_t* d_evals, uint64_t* d_out, void* stream);
 /* The same extension for num_columns columns (a prover's trace columns): column k from
- * d_evals[k] into d_out[k].  For Goldilocks / BabyBear the columns run back to back on one
- * stream sharing the shift's power tables and the scratch, with one wait at the end; for
- * the 256-bit fields each column is one zntt_coset_lde_device call. */
+ * d_evals[k] into d_out[k].  For Goldilocks / BabyBear every launch covers all columns (a
+ * second grid dimension, up to 65535 columns; beyond that, or for one-element inputs, the
+ * columns run one after another), with one wait at the end; for the 256-bit fields each
+ * column is one zntt_coset_lde_device call. */
 int zntt_coset_lde_columns(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t shift[4],
                            const uint64_t* const* d_evals, uint64_t* const* d_out, uint32_t num_columns,
                            void* stream);

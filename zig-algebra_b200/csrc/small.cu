@@ -64,6 +64,7 @@ struct SmallPass {
   const uint64_t* tw;  // twiddle form, stage s at entry 2^s - 1
   uint32_t log_n, S, k, c, first, inverse, tw0_one, scale;
   uint64_t scale_val;  // twiddle form
+  uint32_t src_len;    // column launches' first pass: natural index >= src_len reads as zero
 };
 
 __device__ __forceinline__ uint32_t rev_bits_small(uint32_t x, uint32_t bits) {
@@ -88,14 +89,14 @@ __device__ __forceinline__ void small_butterfly(uint64_t& u, uint64_t& v, bool m
   u = SF::add(u, t);
 }
 
-template <class SF, int LOG_TILE, int THREADS>
-__global__ void __launch_bounds__(THREADS) small_pass_kernel(SmallPass pp) {
+// One tile of one pass.  PAD: the first pass reads natural indices at or
+// beyond pp.src_len as zeros (a zero-padded input that is not stored).
+template <class SF, int LOG_TILE, int THREADS, bool PAD>
+__device__ __forceinline__ void small_pass_body(const SmallPass& pp, uint32_t blk, uint64_t* sm) {
   constexpr uint32_t TILE_MAX = 1u << LOG_TILE;
-  __shared__ uint64_t sm[TILE_MAX];
   const uint32_t k = pp.k, c = pp.c, C = 1u << c;
   const uint32_t tile = 1u << (k + c);
   const uint32_t tid = threadIdx.x;
-  const uint32_t blk = blockIdx.x;
   uint32_t hi_base = 0, m0 = 0, col0 = 0;
   if (pp.first) {
     col0 = blk << c;
@@ -119,7 +120,7 @@ __global__ void __launch_bounds__(THREADS) small_pass_kernel(SmallPass pp) {
         g = hi_base + (row << pp.S) + m0 + col;
         t = row;
       }
-      sm[(t << c) | col] = pp.src[g];
+      sm[(t << c) | col] = (PAD && pp.first && g >= pp.src_len) ? 0 : pp.src[g];
     }
   }
   __syncthreads();
@@ -198,6 +199,24 @@ __global__ void __launch_bounds__(THREADS) small_pass_kernel(SmallPass pp) {
   }
 }
 
+template <class SF, int LOG_TILE, int THREADS>
+__global__ void __launch_bounds__(THREADS) small_pass_kernel(SmallPass pp) {
+  __shared__ uint64_t sm[1u << LOG_TILE];
+  small_pass_body<SF, LOG_TILE, THREADS, false>(pp, blockIdx.x, sm);
+}
+
+// The same pass over many columns of one size: column blockIdx.y reads
+// srcs[y] and writes dsts[y] (device pointer tables).
+template <class SF, int LOG_TILE, int THREADS>
+__global__ void __launch_bounds__(THREADS) small_pass_cols_kernel(SmallPass pp, const uint64_t* const* srcs,
+                                                                  uint64_t* const* dsts) {
+  __shared__ uint64_t sm[1u << LOG_TILE];
+  SmallPass q = pp;
+  q.src = srcs[blockIdx.y];
+  q.dst = dsts[blockIdx.y];
+  small_pass_body<SF, LOG_TILE, THREADS, true>(q, blockIdx.x, sm);
+}
+
 // Flat table entry e = 2^s - 1 + j holds root^(j * 2^(log_n - 1 - s)), in
 // twiddle form, from three power tables pw[t][i] = root^(i * 1024^t).
 template <class SF>
@@ -257,6 +276,19 @@ __global__ void small_pointwise_kernel(const uint64_t* a, const uint64_t* __rest
     out[i] = SF::mul(SF::mul(a[i], r2), b[i]);
 }
 
+// The coset step over m contiguous columns of 2^log_n values each: element
+// i of every column times shift^i (i < 2^30, power tables as above).
+template <class SF>
+__global__ void small_coset_scale_cols_kernel(const uint64_t* __restrict__ pw, uint64_t* __restrict__ data,
+                                              uint64_t total, uint32_t log_n) {
+  const uint64_t mask = (1ull << log_n) - 1;
+  for (uint64_t f = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; f < total; f += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = f & mask;
+    const uint64_t v = SF::mul(__ldg(pw + (i & 1023)), __ldg(pw + 1024 + ((i >> 10) & 1023)));
+    data[f] = SF::mul(SF::mul(v, __ldg(pw + 2048 + (i >> 20))), data[f]);
+  }
+}
+
 // One FRI fold round (libs/fri/src/root.zig:396-403) on canonical values;
 // half_inv, alpha and the table g^-j / 2 are in twiddle form.
 template <class SF>
@@ -285,6 +317,16 @@ cudaError_t launch_small_pass(int field, const SmallPass& pp, uint64_t tiles, cu
     small_pass_kernel<Goldilocks, kSmallLogTile, kSmallThreads><<<(unsigned)tiles, kSmallThreads, 0, st>>>(pp);
   else
     small_pass_kernel<BabyBear, kSmallLogTile, kSmallThreads><<<(unsigned)tiles, kSmallThreads, 0, st>>>(pp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_small_pass_cols(int field, const SmallPass& pp, uint64_t tiles, uint32_t m,
+                                   const uint64_t* const* srcs, uint64_t* const* dsts, cudaStream_t st) {
+  const dim3 grid((unsigned)tiles, m);
+  if (field == kGoldilocksField)
+    small_pass_cols_kernel<Goldilocks, kSmallLogTile, kSmallThreads><<<grid, kSmallThreads, 0, st>>>(pp, srcs, dsts);
+  else
+    small_pass_cols_kernel<BabyBear, kSmallLogTile, kSmallThreads><<<grid, kSmallThreads, 0, st>>>(pp, srcs, dsts);
   return cudaGetLastError();
 }
 
@@ -531,6 +573,33 @@ SmallRegistration* small_find_registration(int field, uint32_t log_n, const zntt
 
 // src -> dst over 2^log_n device elements; scratch (2^log_n) is needed when
 // src == dst and there are several passes.
+// small_run over m columns at once: the first pass reads srcs[y] (zero beyond
+// src_len) and writes dsts[y]; the later passes run in place on dsts[y], so no
+// scratch is needed.  At least one pass (log_n >= 1).
+int small_run_cols(const SmallTable* t, uint32_t m, const uint64_t* const* srcs, uint64_t* const* dsts,
+                   uint32_t src_len, bool inverse, bool scale, uint64_t scale_tw, cudaStream_t st) {
+  const std::vector<SmallPlanPass> plan = small_plan(t->log_n);
+  for (size_t p = 0; p < plan.size(); p++) {
+    SmallPass pp;
+    std::memset(&pp, 0, sizeof(pp));
+    pp.tw = t->d_table;
+    pp.log_n = t->log_n;
+    pp.S = plan[p].S;
+    pp.k = plan[p].k;
+    pp.c = plan[p].c;
+    pp.first = p == 0;
+    pp.inverse = inverse;
+    pp.tw0_one = t->tw0_one;
+    pp.scale = p + 1 == plan.size() && scale;
+    pp.scale_val = scale_tw;
+    pp.src_len = src_len;
+    const uint64_t tiles = (1ull << t->log_n) >> (pp.k + pp.c);
+    cudaError_t ce = launch_small_pass_cols(t->field, pp, tiles, m, p == 0 ? srcs : dsts, dsts, st);
+    if (ce != cudaSuccess) return cuda_fail(ce, "small-field pass");
+  }
+  return ZNTT_OK;
+}
+
 int small_run(const SmallTable* t, const uint64_t* src, uint64_t* dst, uint64_t* scratch, bool inverse, bool scale,
               uint64_t scale_tw, cudaStream_t st) {
   const std::vector<SmallPlanPass> plan = small_plan(t->log_n);
@@ -1009,6 +1078,54 @@ int small_coset_lde_many(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out
   void* d_pw = nullptr;
   int rc = pool_get(pw.size() * 8, &d_pw);
   if (rc) return rc;
+  if (ti->log_n >= 1 && m <= 65535) {
+    // All columns per launch: the inverse transforms into a contiguous buffer of
+    // m x 2^log_in coefficients, one coset-scaling launch over it, and the
+    // forward transforms reading it zero-padded to 2^log_out, with the column
+    // picked by blockIdx.y from device pointer tables.
+    const size_t tmp_bytes = (size_t)m * n_in * 8, tab_bytes = (size_t)3 * m * 8;
+    void* tmp = nullptr;
+    void* tabs = nullptr;
+    rc = pool_get(tmp_bytes, &tmp);
+    if (!rc) rc = pool_get(tab_bytes, &tabs);
+    if (rc) {
+      if (tmp) pool_put(tmp, tmp_bytes);
+      pool_put(d_pw, pw.size() * 8);
+      return rc;
+    }
+    std::vector<const void*> h(3 * (size_t)m);
+    for (uint32_t k = 0; k < m; k++) {
+      h[k] = d_evals[k];
+      h[m + k] = static_cast<uint64_t*>(tmp) + (size_t)k * n_in;
+      h[2 * (size_t)m + k] = d_out[k];
+    }
+    const uint64_t* const* t_src = static_cast<const uint64_t* const*>(tabs);
+    uint64_t* const* t_tmp = static_cast<uint64_t* const*>(tabs) + m;
+    uint64_t* const* t_out = static_cast<uint64_t* const*>(tabs) + 2 * (size_t)m;
+    cudaError_t ce = cudaMemcpyAsync(d_pw, pw.data(), pw.size() * 8, cudaMemcpyHostToDevice, st);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(tabs, h.data(), tab_bytes, cudaMemcpyHostToDevice, st);
+    if (ce == cudaSuccess) {
+      rc = small_run_cols(ti, m, t_src, t_tmp, (uint32_t)n_in, true, true, n_inverse_tw(H, ti->log_n), st);
+      if (rc == ZNTT_OK) {
+        if (ti->field == kGoldilocksField)
+          small_coset_scale_cols_kernel<Goldilocks><<<grid_for((uint64_t)m * n_in), 256, 0, st>>>(
+              (const uint64_t*)d_pw, static_cast<uint64_t*>(tmp), (uint64_t)m * n_in, ti->log_n);
+        else
+          small_coset_scale_cols_kernel<BabyBear><<<grid_for((uint64_t)m * n_in), 256, 0, st>>>(
+              (const uint64_t*)d_pw, static_cast<uint64_t*>(tmp), (uint64_t)m * n_in, ti->log_n);
+        ce = cudaGetLastError();
+        if (ce == cudaSuccess) rc = small_run_cols(to, m, t_tmp, t_out, (uint32_t)n_in, false, false, 0, st);
+      }
+    }
+    cudaError_t ce2 = cudaStreamSynchronize(st);  // the buffers return to the pool after the stream is done
+    pool_put(d_pw, pw.size() * 8);
+    pool_put(tmp, tmp_bytes);
+    pool_put(tabs, tab_bytes);
+    if (rc) return rc;
+    if (ce == cudaSuccess) ce = ce2;
+    if (ce != cudaSuccess) return cuda_fail(ce, "coset extension");
+    return ZNTT_OK;
+  }
   void* scratch = nullptr;
   const size_t sbytes = (size_t)8 << to->log_n;
   rc = pool_get(sbytes, &scratch);
@@ -1017,7 +1134,8 @@ int small_coset_lde_many(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out
     return rc;
   }
   // One stream: the columns run one after another and share the power tables and
-  // the forward transform's scratch.
+  // the forward transform's scratch (one-element inputs, or more columns than a
+  // launch's second grid dimension holds).
   cudaError_t ce = cudaMemcpyAsync(d_pw, pw.data(), pw.size() * 8, cudaMemcpyHostToDevice, st);
   for (uint32_t k = 0; k < m && ce == cudaSuccess && rc == ZNTT_OK; k++) {
     uint64_t* out = d_out[k];
