@@ -1040,11 +1040,13 @@ extern "C" int zntt_bit_reverse_small(uint64_t* data, size_t len) {
 
 namespace zntt {
 
-// The coset low-degree extension for a small field, the composition the
-// 256-bit path runs in its fused passes, as separate device steps: the
-// inverse transform of the 2^log_in evaluations into the head of d_out (with
-// 1/n), coefficient i times shift^i, the tail zeroed, and the forward
-// transform of d_out in place.
+// The coset low-degree extension of m columns for a small field, the
+// composition the 256-bit path runs in its fused passes, as device steps:
+// the inverse transform of each column's 2^log_in evaluations (with 1/n),
+// coefficient i times shift^i, and the forward transform of the coefficients
+// zero-padded to 2^log_out.  Every launch covers all columns (below); inputs
+// of one element, or more columns than a grid's second dimension, take the
+// per-column path at the end.
 int small_coset_lde_many(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t* shift,
                          const uint64_t* const* d_evals, uint64_t* const* d_out, uint32_t m, void* stream) {
   const SmallTable* ti = reinterpret_cast<const SmallTable*>(tw_in);
