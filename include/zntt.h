@@ -139,6 +139,13 @@ enum zntt_mode {
 int zntt_ntt_device(const zntt_twiddles* tw, const uint64_t* d_src, uint64_t* d_dst, uint64_t* d_scratch,
                     int mode, void* stream);
 
+/* Forward or inverse transforms of num_columns device columns of 2^log_n elements (the
+ * table's size), column k from d_src[k] into d_dst[k], out of place.  For Goldilocks /
+ * BabyBear every launch covers all columns (up to 65535) and the call waits for its stream;
+ * for the 256-bit fields each column is one zntt_ntt_device call (stream-ordered). */
+int zntt_ntt_device_columns(const zntt_twiddles* tw, const uint64_t* const* d_src, uint64_t* const* d_dst,
+                            uint32_t num_columns, int mode, void* stream);
+
 /* In-place transform of the 2^log_n device elements at d_data (log_n of the
  * twiddle handle, at most 18) that allocates no memory.  No counterpart in the
  * reference.  For callers that must not allocate device memory when they

@@ -265,3 +265,34 @@ def test_coset_lde_columns_equal_single_extensions(z):
         torch.cuda.synchronize()
         for k, (o, w) in enumerate(zip(outs, wants)):
             assert torch.equal(o, w), (F.name, k)
+
+
+@pytest.mark.parametrize("log_n", [0, 1, 10, 13, 20])
+def test_ntt_device_columns_equal_single_transforms(z, log_n):
+    """zntt_ntt_device_columns (every launch over all columns) equals one zntt_ntt_device call
+    per column, forward and inverse, for the small fields and BN254-Fr; in place is refused."""
+    torch = pytest.importorskip("torch")
+    for F, fid, m in [(z.GOLDILOCKS, O.GOLDILOCKS, 5), (z.BABYBEAR, O.BABYBEAR, 3), (z.BN254_FR, O.BN254_FR, 2)]:
+        n = 1 << log_n
+        if F.limbs == 4 and log_n == 0:
+            continue  # the 256-bit path is one zntt_ntt_device call per column, covered elsewhere
+        if F.limbs == 4:
+            cols = [torch.from_numpy(O.random_elements(fid, 70 + k, n).view(np.int64).reshape(-1).copy()).cuda()
+                    for k in range(m)]
+        else:
+            cols = [torch.from_numpy(_random(fid, 70 + k, n).view(np.int64).copy()).cuda() for k in range(m)]
+        torch.cuda.synchronize()
+        with z.DeviceTwiddles(F, log_n, z.primitiveRootOfUnity(F, log_n)) as t:
+            for mode in (z.FORWARD, z.INVERSE):
+                outs = [torch.empty_like(c) for c in cols]
+                wants = [torch.empty_like(c) for c in cols]
+                torch.cuda.synchronize()
+                z.ntt_device_columns(t, [c.data_ptr() for c in cols], [o.data_ptr() for o in outs], mode)
+                for c, w in zip(cols, wants):
+                    z.ntt_device(t, c.data_ptr(), w.data_ptr(), mode)
+                torch.cuda.synchronize()
+                for k, (o, w) in enumerate(zip(outs, wants)):
+                    assert torch.equal(o, w), (F.name, log_n, mode, k)
+            if F.limbs == 1 and log_n > 0:
+                with pytest.raises(z.InvalidArgument):
+                    z.ntt_device_columns(t, [cols[0].data_ptr()], [cols[0].data_ptr()])

@@ -200,6 +200,7 @@ def lib():
         L.zntt_twiddles_acquire.argtypes = [i, ctypes.c_uint32, _U64P, ctypes.POINTER(vp)]
         L.zntt_twiddles_release.argtypes = [vp]
         L.zntt_ntt_device.argtypes = [vp, vp, vp, vp, i, vp]
+        L.zntt_ntt_device_columns.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_uint32, i, vp]
         L.zntt_random_elements.argtypes = [i, ctypes.c_char_p, vp, sz, vp]
         L.zntt_elementwise_device.argtypes = [i, i, vp, vp, vp, sz, vp]
         L.zntt_probe_imad.argtypes = [ctypes.POINTER(ctypes.c_double)]
@@ -435,6 +436,15 @@ def ntt_device(tw: DeviceTwiddles, d_src: int, d_dst: int, mode: int = FORWARD, 
                stream: int = 0) -> None:
     """Transforms 2^tw.log_n device elements (pointers as ints) on `stream`."""
     _check(lib().zntt_ntt_device(tw.handle, d_src, d_dst, d_scratch or None, mode, stream or None))
+
+
+def ntt_device_columns(tw: DeviceTwiddles, d_srcs, d_dsts, mode: int = FORWARD, stream: int = 0) -> None:
+    """Transforms of several device columns of the table's size, out of place
+    (zntt_ntt_device_columns)."""
+    m = len(d_srcs)
+    src = (ctypes.c_void_p * max(m, 1))(*d_srcs)
+    dst = (ctypes.c_void_p * max(len(d_dsts), 1))(*d_dsts)
+    _check(lib().zntt_ntt_device_columns(tw.handle, src, dst, m, mode, stream or None))
 
 
 def ntt_device_inplace_noalloc(tw: DeviceTwiddles, d_data: int, mode: int = FORWARD, stream: int = 0) -> None:

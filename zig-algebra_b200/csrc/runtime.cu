@@ -770,6 +770,23 @@ int zntt_twiddles_release(zntt_twiddles* tw) {
   return ZNTT_OK;
 }
 
+int zntt_ntt_device_columns(const zntt_twiddles* tw, const uint64_t* const* d_src, uint64_t* const* d_dst,
+                            uint32_t num_columns, int mode, void* stream) {
+  clear_error();
+  if (!tw || !d_src || !d_dst) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null pointer");
+  if (num_columns == 0) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "no columns");
+  if (mode != ZNTT_FORWARD && mode != ZNTT_INVERSE) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "unknown mode");
+  int rc = check_init();
+  if (rc) return rc;
+  if (is_small_table(tw)) return small_ntt_columns(tw, d_src, d_dst, num_columns, mode, stream);
+  for (uint32_t k = 0; k < num_columns; k++) {  // 256-bit fields: one transform per column
+    if (!d_src[k] || !d_dst[k]) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null column");
+    rc = zntt_ntt_device(tw, d_src[k], d_dst[k], nullptr, mode, stream);
+    if (rc) return rc;
+  }
+  return ZNTT_OK;
+}
+
 int zntt_ntt_device(const zntt_twiddles* tw, const uint64_t* d_src, uint64_t* d_dst, uint64_t* d_scratch, int mode,
                     void* stream) {
   clear_error();

@@ -1257,3 +1257,56 @@ int small_poly_mul(int field, const uint64_t* a, size_t a_len, const uint64_t* b
 }
 
 }  // namespace zntt
+
+namespace zntt {
+
+// Forward or inverse transforms of m columns of one size, out of place, every
+// launch covering all columns (small_pass_cols_kernel).  Synchronous: the
+// device pointer tables return to the pool when the stream is done.
+int small_ntt_columns(const zntt_twiddles* tw, const uint64_t* const* d_src, uint64_t* const* d_dst, uint32_t m,
+                      int mode, void* stream) {
+  const SmallTable* t = reinterpret_cast<const SmallTable*>(tw);
+  const SmallHost& H = small_host(t->field);
+  const uint64_t n = 1ull << t->log_n;
+  if (m > 65535) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "at most 65535 columns per call");
+  for (uint32_t k = 0; k < m; k++) {
+    if (!d_src[k] || !d_dst[k]) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null column");
+    const char* a = reinterpret_cast<const char*>(d_src[k]);
+    const char* b = reinterpret_cast<const char*>(d_dst[k]);
+    if (a < b + n * 8 && b < a + n * 8)
+      return set_error(ZNTT_ERR_INVALID_ARGUMENT, "a column's output overlaps its input (columns run out of place)");
+  }
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+  const bool inverse = mode == ZNTT_INVERSE;
+  cudaError_t ce = cudaSuccess;
+  if (t->log_n == 0) {  // one element per column: a copy (the 1/n scale is by one)
+    for (uint32_t k = 0; k < m && ce == cudaSuccess; k++)
+      ce = cudaMemcpyAsync(d_dst[k], d_src[k], 8, cudaMemcpyDeviceToDevice, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) return cuda_fail(ce, "copy");
+    return ZNTT_OK;
+  }
+  const size_t tab_bytes = (size_t)2 * m * 8;
+  void* tabs = nullptr;
+  int rc = pool_get(tab_bytes, &tabs);
+  if (rc) return rc;
+  std::vector<const void*> h(2 * (size_t)m);
+  for (uint32_t k = 0; k < m; k++) {
+    h[k] = d_src[k];
+    h[m + k] = d_dst[k];
+  }
+  ce = cudaMemcpyAsync(tabs, h.data(), tab_bytes, cudaMemcpyHostToDevice, st);
+  if (ce == cudaSuccess)
+    rc = small_run_cols(t, m, static_cast<const uint64_t* const*>(tabs), static_cast<uint64_t* const*>(tabs) + m,
+                        (uint32_t)n, inverse, inverse, inverse ? n_inverse_tw(H, t->log_n) : 0, st);
+  cudaError_t ce2 = cudaStreamSynchronize(st);
+  pool_put(tabs, tab_bytes);
+  if (rc) return rc;
+  if (ce == cudaSuccess) ce = ce2;
+  if (ce != cudaSuccess) return cuda_fail(ce, "column transforms");
+  return ZNTT_OK;
+}
+
+}  // namespace zntt

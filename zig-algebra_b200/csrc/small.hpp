@@ -36,6 +36,8 @@ int small_fold_params(int field, uint32_t log_table, const uint64_t* alpha, cons
 int wide_fold_params(int field, uint32_t log_table, const void** tab_out, uint32_t half_inv[8]);
 int small_poly_mul(int field, const uint64_t* a, size_t a_len, const uint64_t* b, size_t b_len, size_t max_degree,
                    uint64_t* out, int64_t* out_degree);
+int small_ntt_columns(const zntt_twiddles* tw, const uint64_t* const* d_src, uint64_t* const* d_dst, uint32_t m,
+                      int mode, void* stream);
 int small_coset_lde_many(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t* shift,
                          const uint64_t* const* d_evals, uint64_t* const* d_out, uint32_t m, void* stream);
 int small_coset_lde(const zntt_twiddles* tw_in, const zntt_twiddles* tw_out, const uint64_t* shift,
