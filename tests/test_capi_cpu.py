@@ -169,6 +169,20 @@ def test_small_field_poly_mul_contract_before_any_device_work(zntt):
             zntt.poly_mul(F, np.array([F.modulus], dtype=np.uint64), b, 10)
 
 
+def test_column_entry_points_check_arguments_first(zntt):
+    """The many-column entry points refuse null pointers, zero columns and unknown modes before
+    they look at a table or a device."""
+    L = zntt.lib()
+    one = (ctypes.c_void_p * 1)(1 << 20)
+    for args in ((None, one, one, 1, 0), (1, None, one, 1, 0), (1, one, one, 0, 0), (1, one, one, 1, 7)):
+        with pytest.raises(zntt.InvalidArgument):
+            zntt._check(L.zntt_ntt_device_columns(*args, None))
+    shift = (ctypes.c_uint64 * 4)(7, 0, 0, 0)
+    for args in ((None, 1, shift, one, one, 1), (1, 1, shift, None, one, 1), (1, 1, shift, one, one, 0)):
+        with pytest.raises(zntt.InvalidArgument):
+            zntt._check(L.zntt_coset_lde_columns(*args, None))
+
+
 def test_small_fields_host_side(zntt, oracle):
     """Goldilocks and BabyBear: field info, primitive roots as zig-field derives them (the
     roots of the reference's KAT, libs/ntt/src/root.zig:437-447, and the oracle's at every
