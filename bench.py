@@ -13,10 +13,14 @@ host vectors, whose timed region includes every step's host->device copy of
 the input and device->host copy of the result (overlapped across vectors), and
 beside it one synchronous zntt_ntt_with_twiddles call.  Under torchrun every
 rank transforms its own vector (independent objects: weak scaling, no
-collective on the data path); the time is the max over ranks.  The default run
-adds, on rank 0, one key per configuration beside the headline (batched,
-coset_lde, poly_mul, small_fields, fri_fold); --workload prints one of them
-alone as its own line, and `serve` replays the request trace.
+collective on the data path); the time is the max over ranks.  `e2e.pcie`
+measures the host link's duplex bound beside it.  The default run adds, on
+rank 0, one key per configuration beside the headline (batched, coset_lde,
+poly_mul, small_fields -- transforms, an extension, a 64-column trace extension
+and row commitment -- and fri_fold -- folds, layer and row commitments against
+the BLAKE3 probe, the prover loop and its openings, for BN254-Fr, Goldilocks and
+BabyBear); --workload prints one of them alone as its own line, and `serve`
+replays the request trace.
 
 `--impl reference` times the CPU restatement of zig-ntt (oracle/) on all host
 cores instead: zig-ntt has no GPU path and its toolchain (Zig 0.16) is not
