@@ -82,6 +82,11 @@ int zntt_init(int device);
 int zntt_shutdown(void);
 /* Message of the last failure on the calling thread ("" when none). */
 const char* zntt_last_error(void);
+/* The library's device buffer pool: buffers taken from it (scratch and staging
+ * of the transforms), cudaMalloc calls it made, and idle bytes it caches.  For
+ * callers that watch device memory, and for tests that check an entry point
+ * allocates nothing.  No counterpart in the reference. */
+int zntt_pool_stats(uint64_t* acquires, uint64_t* device_mallocs, uint64_t* cached_bytes);
 /* Modulus (canonical, 4 LE limbs) and two-adicity of a field. */
 int zntt_field_info(int field, uint64_t modulus[4], uint32_t* two_adicity);
 /* F.primitiveRootOfUnity(log_n) in Montgomery form: the first quadratic
@@ -197,6 +202,15 @@ int zntt_batch_run(zntt_batch* b, void* stream);
 int zntt_batch_run_graph(zntt_batch* b, void* stream);
 /* After the stream finished: ZNTT_OK, or ZNTT_ERR_TIMEOUT if a wait gave up. */
 int zntt_batch_status(zntt_batch* b);
+/* How many sleep rounds (about 0.25-1 us each) a tile waits for its job's
+ * previous pass before it raises the batch's error flag (after which every CTA
+ * stops at its next item and zntt_batch_status reports ZNTT_ERR_TIMEOUT).
+ * Default ZNTT_BATCH_SPIN_LIMIT; 0 makes any wait give up at once, which is
+ * how a test drives the timeout path without faulting anything.  Takes effect
+ * at the next run (a captured graph is re-captured).  No counterpart in the
+ * reference, which has no device waits. */
+#define ZNTT_BATCH_SPIN_LIMIT 4194304u
+int zntt_batch_set_spin_limit(zntt_batch* b, uint32_t spin_limit);
 int zntt_batch_info(const zntt_batch* b, uint32_t* n_items, uint32_t* n_passes, int* grid, int* shape);
 int zntt_batch_destroy(zntt_batch* b);
 

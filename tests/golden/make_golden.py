@@ -267,8 +267,12 @@ def merkle_rows_cases() -> dict:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("ZIG_ALGEBRA_SRC"),
+                    help="the zig-algebra source tree the known answers are read from "
+                         "(default: $ZIG_ALGEBRA_SRC)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference or set ZIG_ALGEBRA_SRC to the zig-algebra source tree")
     json.dump(parse_kats(args.reference), open(os.path.join(HERE, "ntt_kat.json"), "w"), indent=1)
     json.dump(parse_rfc(args.reference), open(os.path.join(HERE, "chacha20_rfc8439.json"), "w"), indent=1)
     json.dump(fr_cases(), open(os.path.join(HERE, "fr_transforms.json"), "w"), indent=1)

@@ -216,3 +216,151 @@ def test_every_pass_shape_matches_oracle(z, tmp_path, shape):
                         np.testing.assert_array_equal(_host(y), want, err_msg=f"{F} 2^{L} mode {mode}")
     finally:
         z.tune_clear()
+
+
+# --- the batched configurations against the oracle directly ---------------------------------
+
+def _oracle_jobs(fn, args_list):
+    """Runs oracle calls (each single-threaded) on all host cores; ctypes releases the GIL."""
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=WORKERS) as ex:
+        return list(ex.map(lambda a: fn(*a), args_list))
+
+
+class OracleTables:
+    """The oracle's precomputeTwiddles stages of the primitive 2^log_n-th root, per log n."""
+
+    def __init__(self, fid):
+        self.fid, self.t = fid, {}
+
+    def __call__(self, log_n):
+        if log_n not in self.t:
+            st, root = O.primitive_root(self.fid, log_n)
+            assert st == O.OK
+            st, stages = O.precompute_twiddles(self.fid, log_n, root)
+            assert st == O.OK
+            self.t[log_n] = stages
+        return self.t[log_n]
+
+
+def test_mixed_batch_of_the_benchmark_matches_oracle(z):
+    """The batched configuration itself -- 512 BN254-Fr transforms of 2^U{10..16} plus 8 of 2^20,
+    directions 50/50 by seed, in one persistent launch (plain and through the CUDA graph) --
+    equals the oracle's nttWithTwiddles / inttWithTwiddles (libs/ntt/src/root.zig:148-212) for
+    every job."""
+    torch = _torch()
+    F, fid = z.BN254_FR, O.BN254_FR
+    rng = np.random.default_rng(33)
+    logs = [int(v) for v in rng.integers(10, 17, 512)] + [20] * 8
+    modes = [z.INVERSE if v < 0.5 else z.FORWARD for v in rng.random(len(logs))]
+    total = sum(1 << L for L in logs)
+    pool = torch.empty(total * 4, dtype=torch.int64, device="cuda")
+    z.random_elements(F, 33, pool.data_ptr(), total)
+    host = _host(pool)
+    tabs, otabs = Tables(z, F), OracleTables(fid)
+    jobs, outs, offs = [], [], []
+    off = 0
+    for L, m in zip(logs, modes):
+        y = torch.empty((1 << L) * 4, dtype=torch.int64, device="cuda")
+        jobs.append({"kind": z.JOB_NTT, "tw": tabs(L), "mode": m, "src": pool.data_ptr() + off * 32,
+                     "dst": y.data_ptr()})
+        outs.append(y)
+        offs.append(off)
+        off += 1 << L
+
+    def oracle_job(i):
+        L = logs[i]
+        want = np.ascontiguousarray(host[offs[i]:offs[i] + (1 << L)])
+        assert O.ntt_with_twiddles(fid, want, L, otabs(L), inverse=modes[i] == z.INVERSE, inplace4=True) == O.OK
+        return want
+
+    for L in sorted(set(logs)):
+        otabs(L)  # tables built once, before the threads share them
+    wants = _oracle_jobs(oracle_job, [(i,) for i in range(len(logs))])
+    with z.Batch(F, jobs) as b:
+        assert b.info()["items"] > 30000
+        for graph in (False, True, True):
+            for y in outs:
+                y.zero_()
+            torch.cuda.synchronize()
+            b.run(graph=graph)
+            torch.cuda.synchronize()
+            b.status()
+            for i, (y, want) in enumerate(zip(outs, wants)):
+                np.testing.assert_array_equal(_host(y), want, err_msg=f"job {i}: 2^{logs[i]} mode {modes[i]} "
+                                                                      f"graph {graph}")
+    tabs.close()
+
+
+def test_batched_coset_extensions_of_the_benchmark_match_oracle(z):
+    """The batched coset-extension configuration: 64 BLS12-381-Fr extensions 2^18 -> 2^20 with
+    g = 5 in one persistent launch, every one equal to the oracle's composition of
+    inttWithTwiddles, zero padding, powers/hadamard (libs/poly/src/vector.zig:24-32,68-73) and
+    nttWithTwiddles."""
+    torch = _torch()
+    F, fid = z.BLS12_381_FR, O.BLS12_381_FR
+    shift = O.from_int(fid, 5)
+    tabs = Tables(z, F)
+    pool = torch.empty(64 * (1 << 18) * 4, dtype=torch.int64, device="cuda")
+    z.random_elements(F, 44, pool.data_ptr(), 64 << 18)
+    host = _host(pool)
+    outs = [torch.empty((1 << 20) * 4, dtype=torch.int64, device="cuda") for _ in range(64)]
+    jobs = [{"kind": z.JOB_COSET_LDE, "tw": tabs(20), "tw_in": tabs(18), "shift": shift,
+             "src": pool.data_ptr() + i * (32 << 18), "dst": outs[i].data_ptr()} for i in range(64)]
+    wants = _oracle_jobs(lambda i: O.coset_lde(fid, np.ascontiguousarray(host[i << 18:(i + 1) << 18]), 18, 2, shift),
+                         [(i,) for i in range(64)])
+    with z.Batch(F, jobs) as b:
+        for graph in (False, True):
+            for y in outs:
+                y.zero_()
+            torch.cuda.synchronize()
+            b.run(graph=graph)
+            torch.cuda.synchronize()
+            b.status()
+            for i, (y, want) in enumerate(zip(outs, wants)):
+                np.testing.assert_array_equal(_host(y), want, err_msg=f"extension {i} graph {graph}")
+    tabs.close()
+
+
+def test_bounded_wait_times_out_then_batch_recovers(z):
+    """The persistent kernel's dependency wait is bounded.  With a limit of zero rounds the
+    first tile that finds its previous pass unfinished raises the batch's error flag: the
+    launch still completes, every CTA stops at its next item, and status() reports Timeout.
+    With the default limit restored the same batch (plain and graph) is bit-exact again."""
+    torch = _torch()
+    F, fid = z.BN254_FR, O.BN254_FR
+    tabs, otabs = Tables(z, F), OracleTables(fid)
+    # One multi-pass job: its second pass's first tile is taken while the first pass's last
+    # wave of tiles is still running on the other CTAs, so that wait cannot find it done.
+    logs = [21]
+    xs = [_vec(z, F, 6100 + i, 1 << L) for i, L in enumerate(logs)]
+    ys = [torch.empty_like(x) for x in xs]
+    jobs = [{"kind": z.JOB_NTT, "tw": tabs(L), "mode": z.FORWARD, "src": x.data_ptr(), "dst": y.data_ptr()}
+            for L, x, y in zip(logs, xs, ys)]
+
+    def oracle_job(i):
+        want = _host(xs[i])
+        assert O.ntt_with_twiddles(fid, want, logs[i], otabs(logs[i]), inplace4=True) == O.OK
+        return want
+
+    for L in set(logs):
+        otabs(L)
+    wants = _oracle_jobs(oracle_job, [(i,) for i in range(len(logs))])
+    with z.Batch(F, jobs) as b:
+        assert b.info()["passes"] > len(jobs) and b.info()["items"] > 2 * b.info()["grid"]
+        for graph in (False, True):
+            b.set_spin_limit(0)
+            torch.cuda.synchronize()
+            b.run(graph=graph)
+            torch.cuda.synchronize()  # the launch ends: no CTA waits without a bound
+            with pytest.raises(z.Timeout):
+                b.status()
+            b.set_spin_limit(z.BATCH_SPIN_LIMIT)
+            for y in ys:
+                y.zero_()
+            b.run(graph=graph)
+            torch.cuda.synchronize()
+            b.status()
+            for i, (y, want) in enumerate(zip(ys, wants)):
+                np.testing.assert_array_equal(_host(y), want, err_msg=f"job {i} after the timeout, graph {graph}")
+    tabs.close()

@@ -214,6 +214,43 @@ def test_errors_leave_data_untouched(z):
     z.freeTwiddles(F, tw)
 
 
+@pytest.mark.parametrize("log_n", [10, 11, 16, 21])
+def test_lazy_reduction_bounds(z, log_n):
+    """Inputs and caller tables that push every butterfly to its bounds.  BN254-Fr keeps values in
+    [0, 2p) inside a pass and skips each product's final subtraction; with every element and
+    every twiddle at p - 1 (raw limbs, so tw[s][0] != 1 and every butterfly multiplies) the sums
+    and differences meet 2p - 2 and the products their largest inputs.  Also alternating 0 / p - 1
+    data, and p - 1 data against tables of 1 and of Montgomery one.  Under the default plan
+    (2^11-element tiles, at most 10 stages per pass) 2^10 and 2^11 run one pass, 2^16 two and
+    2^21 three, so every pass boundary's reduction to [0, p) is crossed.  Both directions,
+    nttWithTwiddles / inttWithTwiddles (libs/ntt/src/root.zig:148-212; the arithmetic is
+    libs/field/src/montgomery.zig:197-297), against the oracle bit for bit."""
+    n = 1 << log_n
+    for F, fid in _fields(z):
+        p = O.MODULI[fid]
+        pm1 = np.array(O.int_to_limbs(p - 1), dtype=np.uint64)
+        one = np.array(O.int_to_limbs(1), dtype=np.uint64)
+        mont_one = O.from_int(fid, 1)
+        zero = np.zeros(4, dtype=np.uint64)
+
+        def filled(v, count):
+            return np.ascontiguousarray(np.tile(v, (count, 1)))
+
+        alternating = np.ascontiguousarray(np.where((np.arange(n) % 2 == 0)[:, None], zero, pm1))
+        cases = [("p-1 data, p-1 table", filled(pm1, n), pm1),
+                 ("alternating 0/p-1 data, p-1 table", alternating, pm1),
+                 ("p-1 data, table of 1", filled(pm1, n), one),
+                 ("p-1 data, table of Montgomery one", filled(pm1, n), mont_one)]
+        for name, x, tv in cases:
+            table = [filled(tv, 1 << s) for s in range(log_n)]
+            for inverse in (False, True):
+                got, want = x.copy(), x.copy()
+                (z.inttWithTwiddles if inverse else z.nttWithTwiddles)(F, got, log_n, table)
+                assert O.ntt_with_twiddles(fid, want, log_n, table, inverse=inverse, workers=WORKERS,
+                                           inplace4=True) == 0
+                np.testing.assert_array_equal(got, want, err_msg=f"{F} 2^{log_n} {name} inverse={inverse}")
+
+
 def test_convolution_property(z):
     F, fid = z.BLS12_381_FR, O.BLS12_381_FR
     p = O.MODULI[fid]

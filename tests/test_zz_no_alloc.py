@@ -6,8 +6,10 @@ allocator, a latency-critical path -- use this entry point; its scratch is an
 8 MiB array inside the library.  The test calls it through the C ABI twice in a
 row (so the second call starts from the scratch the first one left) and
 checks each result bit-exactly against the existing entry point
-zntt_ntt_device, then checks that a transform larger than the array is
-rejected without touching the data.  Collected last so that a failure here
+zntt_ntt_device, and that the library's buffer pool saw no acquire and made no
+cudaMalloc during the call (so a change that routed this entry point through
+the pool would fail here); then checks that a transform larger than the array
+is rejected without touching the data.  Collected last so that a failure here
 leaves every other test already run.
 """
 from __future__ import annotations
@@ -45,8 +47,12 @@ def test_noalloc_matches_existing_entry_on_consecutive_calls(z, log_n):
                 torch.cuda.synchronize()
                 got = x.clone()
                 torch.cuda.synchronize()
+                before = z.pool_stats()
                 z.ntt_device_inplace_noalloc(tw, got.data_ptr(), mode)
                 torch.cuda.synchronize()
+                after = z.pool_stats()
+                assert after["acquires"] == before["acquires"], "the call took a pool buffer"
+                assert after["device_mallocs"] == before["device_mallocs"], "the call allocated"
                 assert torch.equal(got, want), f"{F} 2^{log_n} call {call}"
 
 

@@ -131,6 +131,7 @@ _U64P = ctypes.POINTER(ctypes.c_uint64)
 _lib = None
 
 JOB_NTT = 0
+BATCH_SPIN_LIMIT = 4194304  # ZNTT_BATCH_SPIN_LIMIT: sleep rounds a batch tile waits for its previous pass
 JOB_COSET_LDE = 1
 JOB_POLY_MUL = 2
 
@@ -212,6 +213,8 @@ def lib():
         L.zntt_batch_run.argtypes = [vp, vp]
         L.zntt_batch_run_graph.argtypes = [vp, vp]
         L.zntt_batch_status.argtypes = [vp]
+        L.zntt_batch_set_spin_limit.argtypes = [vp, ctypes.c_uint32]
+        L.zntt_pool_stats.argtypes = [ctypes.POINTER(ctypes.c_uint64)] * 3
         L.zntt_batch_info.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
                                       ctypes.POINTER(i), ctypes.POINTER(i)]
         L.zntt_batch_destroy.argtypes = [vp]
@@ -481,6 +484,13 @@ def elementwise_device(F: Field, op: str, d_a: int, d_b: int, d_out: int, count:
     _check(lib().zntt_elementwise_device(F.id, code, d_a, d_b or None, d_out, count, stream or None))
 
 
+def pool_stats() -> dict:
+    """The device buffer pool's counters: acquires, cudaMalloc calls and cached idle bytes."""
+    a, m, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    _check(lib().zntt_pool_stats(ctypes.byref(a), ctypes.byref(m), ctypes.byref(c)))
+    return {"acquires": a.value, "device_mallocs": m.value, "cached_bytes": c.value}
+
+
 def probe_imad() -> float:
     _ensure_init()
     v = ctypes.c_double()
@@ -548,6 +558,11 @@ class Batch:
 
     def status(self) -> None:
         _check(lib().zntt_batch_status(self.handle))
+
+    def set_spin_limit(self, spin_limit: int = BATCH_SPIN_LIMIT) -> None:
+        """Rounds a tile waits for its job's previous pass before the batch gives up
+        (Timeout from status()); 0 gives up at the first wait."""
+        _check(lib().zntt_batch_set_spin_limit(self.handle, spin_limit))
 
     def info(self) -> dict:
         ni, npp = ctypes.c_uint32(), ctypes.c_uint32()

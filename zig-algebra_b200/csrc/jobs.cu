@@ -170,7 +170,7 @@ struct zntt_batch {
   size_t ctl_words = 0;
   int grid = 0;
   bool ext = false;  // some pass pads or scales by a table
-  uint32_t spin_limit = 4u << 20;  // x ~0.25-1 us: a stalled dependency gives up after seconds
+  uint32_t spin_limit = ZNTT_BATCH_SPIN_LIMIT;  // x ~0.25-1 us: a stalled dependency gives up after seconds
   std::vector<std::pair<void*, size_t>> scratch;  // pool buffers owned by the batch
   std::vector<CosetTab*> coset_tabs;
   cudaGraph_t graph = nullptr;
@@ -391,6 +391,30 @@ int zntt_batch_status(zntt_batch* b) {
   cudaError_t ce = cudaMemcpy(&flag, b->d_ctl + 1, 4, cudaMemcpyDeviceToHost);
   if (ce != cudaSuccess) return cuda_fail(ce, "batch status");
   if (flag) return set_error(ZNTT_ERR_TIMEOUT, "a batch item waited too long for its prerequisite pass");
+  return ZNTT_OK;
+}
+
+int zntt_batch_set_spin_limit(zntt_batch* b, uint32_t spin_limit) {
+  clear_error();
+  if (!b) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "null batch");
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  if (spin_limit == b->spin_limit) return ZNTT_OK;
+  b->spin_limit = spin_limit;
+  // The limit is a kernel argument: a captured graph holds the old value.
+  // Replays may be in flight on any stream, so the device drains first.
+  if (b->graph_exec || b->graph) {
+    const cudaError_t ce = cudaDeviceSynchronize();
+    if (ce != cudaSuccess) return cuda_fail(ce, "batch spin limit");
+  }
+  if (b->graph_exec) {
+    cudaGraphExecDestroy(b->graph_exec);
+    b->graph_exec = nullptr;
+  }
+  if (b->graph) {
+    cudaGraphDestroy(b->graph);
+    b->graph = nullptr;
+  }
   return ZNTT_OK;
 }
 

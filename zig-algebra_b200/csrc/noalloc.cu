@@ -53,6 +53,10 @@ extern "C" int zntt_ntt_device_inplace_noalloc(const zntt_twiddles* tw, uint64_t
   if (mode != ZNTT_FORWARD && mode != ZNTT_INVERSE) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "unknown mode");
   Context& c = ctx();
   if (c.device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
+  // Held while the table is read and the passes are enqueued, as zntt_ntt_device does, so
+  // that zntt_shutdown or a table eviction on another thread cannot free the table meanwhile.
+  // Enqueueing does not block, so the lock costs the call nothing on the device.
+  std::lock_guard<std::recursive_mutex> ctx_lock(c.mu);
   if (is_small_table(tw))
     return set_error(ZNTT_ERR_UNSUPPORTED_FIELD, "the allocation-free transform takes BN254-Fr or BLS12-381-Fr tables only");
   const TwEntry* e = reinterpret_cast<const TwEntry*>(tw);
@@ -63,8 +67,10 @@ extern "C" int zntt_ntt_device_inplace_noalloc(const zntt_twiddles* tw, uint64_t
   int dev = -1;
   cudaError_t ce = cudaGetDevice(&dev);
   if (ce != cudaSuccess) return cuda_fail(ce, "cudaGetDevice");
-  if (dev != c.device || dev >= kMaxDevices)
+  if (dev != c.device)
     return set_error(ZNTT_ERR_INVALID_ARGUMENT, "the current device is not the one zntt_init selected");
+  if (dev < 0 || dev >= kMaxDevices)
+    return set_error(ZNTT_ERR_INVALID_ARGUMENT, "the allocation-free transform serves device ordinals below 64");
   if (log_n == 0) return ZNTT_OK;  // one element: no stage, and the 1/n scale is by one
 
   uint4* scratch = nullptr;
@@ -79,24 +85,11 @@ extern "C" int zntt_ntt_device_inplace_noalloc(const zntt_twiddles* tw, uint64_t
     scratch = static_cast<uint4*>(g_noalloc_scratch_addr[dev]);
   }
 
-  // Pass plan in a fixed array (the planner's passes never exceed 4 here).
-  PassDesc passes[8];
-  uint32_t np = 0;
-  const uint32_t lt = kShapes[kDefaultShape].log_tile;
-  if (log_n <= lt) {
-    passes[np++] = {0, log_n, 0};
-  } else {
-    const uint32_t kmax = lt - 1, P = (log_n + kmax - 1) / kmax;
-    uint32_t S = 0;
-    for (uint32_t p = 0; p < P && np < 8; p++) {
-      const uint32_t k = log_n / P + (p < log_n % P ? 1 : 0);
-      uint32_t cc = lt - k;
-      const uint32_t lim = p == 0 ? log_n - k : S;
-      if (cc > lim) cc = lim;
-      passes[np++] = {S, k, cc};
-      S += k;
-    }
-  }
+  // The library's planner (a plan is a value; planning allocates nothing): with 2^11-element
+  // tiles and at most 2^18 elements it gives one pass (log_n <= 11) or two.
+  const Plan plan = make_plan(log_n, kDefaultShape, kShapes[kDefaultShape].log_tile - 1);
+  const uint32_t np = plan.np;
+  const PassDesc* passes = plan.p;
 
   uint64_t ninv[4] = {0, 0, 0, 0};
   const bool inverse = mode == ZNTT_INVERSE;

@@ -54,6 +54,7 @@ Context& ctx() {
 // ---------------------------------------------------------------------------
 
 cudaError_t BufferPool::acquire(size_t bytes, void** out) {
+  acquires_++;
   auto it = free_.find(bytes);
   if (it != free_.end()) {
     *out = it->second;
@@ -61,10 +62,12 @@ cudaError_t BufferPool::acquire(size_t bytes, void** out) {
     cached_ -= bytes;
     return cudaSuccess;
   }
+  mallocs_++;
   cudaError_t e = cudaMalloc(out, bytes);
   if (e == cudaErrorMemoryAllocation) {
     cudaGetLastError();
     trim();
+    mallocs_++;
     e = cudaMalloc(out, bytes);
   }
   return e;
@@ -564,6 +567,15 @@ int zntt_shutdown(void) {
 }
 
 const char* zntt_last_error(void) { return g_last_error.c_str(); }
+
+int zntt_pool_stats(uint64_t* acquires, uint64_t* device_mallocs, uint64_t* cached_bytes) {
+  Context& c = ctx();
+  std::lock_guard<std::recursive_mutex> lock(c.mu);
+  if (acquires) *acquires = c.pool.acquires();
+  if (device_mallocs) *device_mallocs = c.pool.device_mallocs();
+  if (cached_bytes) *cached_bytes = c.pool.cached_bytes();
+  return ZNTT_OK;
+}
 
 int zntt_field_info(int field, uint64_t modulus[4], uint32_t* two_adicity) {
   if (is_small_field(field)) return small_field_info(field, modulus, two_adicity);

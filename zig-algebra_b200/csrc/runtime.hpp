@@ -71,10 +71,14 @@ class BufferPool {
   void release(void* p, size_t bytes);
   void trim();
   size_t cached_bytes() const { return cached_; }
+  uint64_t acquires() const { return acquires_; }
+  uint64_t device_mallocs() const { return mallocs_; }
 
  private:
   std::multimap<size_t, void*> free_;
   size_t cached_ = 0;
+  uint64_t acquires_ = 0;  // acquire() calls
+  uint64_t mallocs_ = 0;   // cudaMalloc calls made by acquire()
 };
 
 struct Context {
