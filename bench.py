@@ -15,12 +15,16 @@ beside it one synchronous zntt_ntt_with_twiddles call.  Under torchrun every
 rank transforms its own vector (independent objects: weak scaling, no
 collective on the data path); the time is the max over ranks.  `e2e.pcie`
 measures the host link's duplex bound beside it.  The default run adds, on
-rank 0, one key per configuration beside the headline (batched, coset_lde,
-poly_mul, small_fields -- transforms, an extension, a 64-column trace extension
-and row commitment -- and fri_fold -- folds, layer and row commitments against
-the BLAKE3 probe, the prover loop and its openings, for BN254-Fr, Goldilocks and
-BabyBear); --workload prints one of them alone as its own line, and `serve`
-replays the request trace.
+rank 0, one key per configuration beside the headline: sizes (BN254-Fr 2^20,
+2^22, 2^24 and BLS12-381-Fr 2^24, forward and inverse, each with its fraction of
+the multiply-pipe roofline), batched, coset_lde, poly_mul, small_fields --
+transforms, an extension, a 64-column trace extension and row commitment --,
+fri_fold -- folds, layer and row commitments against the BLAKE3 probe, the
+prover loop and its openings, for BN254-Fr, Goldilocks and BabyBear -- and serve
+(the 20,000-request trace, continuous batching against serial plain launches;
+--no-serve leaves it out).  The line ends with `summary`, a short digest of
+every configuration.  --workload prints one configuration alone as its own line
+(`serve` adds a capacity sweep).
 
 `--impl reference` times the CPU restatement of zig-ntt (oracle/) on all host
 cores instead: zig-ntt has no GPU path and its toolchain (Zig 0.16) is not
