@@ -220,3 +220,15 @@ def test_small_fields_host_side(zntt, oracle):
             zntt.ntt(F, np.zeros((4, 4), dtype=np.uint64), 2, root)
         with pytest.raises(zntt.InvalidTwiddles):
             zntt.nttWithTwiddles(zntt.BN254_FR, np.zeros((2, 4), dtype=np.uint64), 1, [np.zeros(1, dtype=np.uint64)])
+
+
+def test_batch_spin_limit_and_pool_stats_need_no_device(zntt):
+    """zntt_batch_set_spin_limit refuses a null batch before touching anything, and the pool
+    counters read without a device."""
+    L = zntt.lib()
+    assert L.zntt_batch_set_spin_limit(None, 0) == 10  # ZNTT_ERR_INVALID_ARGUMENT
+    assert "null batch" in L.zntt_last_error().decode()
+    st = zntt.pool_stats()
+    assert set(st) == {"acquires", "device_mallocs", "cached_bytes"}
+    assert st["device_mallocs"] <= st["acquires"] * 2
+    assert zntt.BATCH_SPIN_LIMIT == 1 << 22
