@@ -278,7 +278,7 @@ def test_mixed_batch_of_the_benchmark_matches_oracle(z):
         otabs(L)  # tables built once, before the threads share them
     wants = _oracle_jobs(oracle_job, [(i,) for i in range(len(logs))])
     with z.Batch(F, jobs) as b:
-        assert b.info()["items"] > 30000
+        assert b.info()["items"] > 10000  # 16,827 tiles of 2^11 elements under the default plan
         for graph in (False, True, True):
             for y in outs:
                 y.zero_()

@@ -13,25 +13,33 @@
 
 namespace zntt {
 
-template <class F, int LOG_TILE, int THREADS, int MINB, bool EXT>
+template <class F, int LOG_TILE, int THREADS, int MINB, bool EXT, bool FULL>
 __global__ void __launch_bounds__(THREADS, MINB) ntt_pass_kernel(PassParams pp) {
   extern __shared__ uint4 sm[];
-  ntt_tile<F, LOG_TILE, THREADS, false, EXT>(pp, blockIdx.x, sm);
+  ntt_tile<F, LOG_TILE, THREADS, false, EXT, FULL>(pp, blockIdx.x, sm);
 }
 
-template <class F, int SH, bool EXT>
+template <class F, int SH, bool EXT, bool FULL>
 static void* pass_ptr() {
-  return (void*)ntt_pass_kernel<F, kShapes[SH].log_tile, kShapes[SH].threads, kShapes[SH].min_blocks, EXT>;
+  return (void*)ntt_pass_kernel<F, kShapes[SH].log_tile, kShapes[SH].threads, kShapes[SH].min_blocks, EXT, FULL>;
+}
+
+template <class F, int SH>
+static cudaError_t set_shape_attrs() {
+  void* fns[4] = {pass_ptr<F, SH, false, false>(), pass_ptr<F, SH, true, false>(), pass_ptr<F, SH, false, true>(),
+                  pass_ptr<F, SH, true, true>()};
+  for (int i = 0; i < 4; i++) {
+    cudaError_t e = cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize, shape_smem_bytes(SH));
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 template <class F>
 static cudaError_t set_pass_attrs() {
-  void* fns[4] = {pass_ptr<F, 0, false>(), pass_ptr<F, 0, true>(), pass_ptr<F, 1, false>(), pass_ptr<F, 1, true>()};
-  for (int i = 0; i < 4; i++) {
-    cudaError_t e = cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize, shape_smem_bytes(i / 2));
-    if (e != cudaSuccess) return e;
-  }
-  return cudaSuccess;
+  cudaError_t e = set_shape_attrs<F, 0>();
+  if (e == cudaSuccess) e = set_shape_attrs<F, 1>();
+  return e;
 }
 
 cudaError_t configure_kernels() {
@@ -41,13 +49,20 @@ cudaError_t configure_kernels() {
   return configure_batch_kernels();
 }
 
-template <class F, int SH>
-static void launch_pass_shape(bool ext, const PassParams& pp, dim3 grid, cudaStream_t st) {
+template <class F, int SH, bool FULL>
+static void launch_pass_full(bool ext, const PassParams& pp, dim3 grid, cudaStream_t st) {
   constexpr PassShape S = kShapes[SH];
   if (ext)
-    ntt_pass_kernel<F, S.log_tile, S.threads, S.min_blocks, true><<<grid, S.threads, shape_smem_bytes(SH), st>>>(pp);
+    ntt_pass_kernel<F, S.log_tile, S.threads, S.min_blocks, true, FULL><<<grid, S.threads, shape_smem_bytes(SH), st>>>(pp);
   else
-    ntt_pass_kernel<F, S.log_tile, S.threads, S.min_blocks, false><<<grid, S.threads, shape_smem_bytes(SH), st>>>(pp);
+    ntt_pass_kernel<F, S.log_tile, S.threads, S.min_blocks, false, FULL><<<grid, S.threads, shape_smem_bytes(SH), st>>>(pp);
+}
+
+template <class F, int SH>
+static void launch_pass_shape(bool ext, const PassParams& pp, dim3 grid, cudaStream_t st) {
+  // Passes whose tile is the shape's whole tile run the variant without bound checks.
+  if (pp.k + pp.c == (uint32_t)kShapes[SH].log_tile) launch_pass_full<F, SH, true>(ext, pp, grid, st);
+  else launch_pass_full<F, SH, false>(ext, pp, grid, st);
 }
 
 template <class F>

@@ -83,12 +83,15 @@ __device__ __forceinline__ uint4 load_data(const uint4* p) {
 // EXT enables the extension features: zero padding of the first pass's input
 // from index src_len, a per-position scale table, and storing only the output
 // positions below dst_len.  Plain transforms compile without them (fewer live
-// registers in the hot loop).
-template <class F, int LOG_TILE, int THREADS, bool COHERENT, bool EXT>
+// registers in the hot loop).  FULL: the tile is the shape's whole tile
+// (k + c == LOG_TILE, every pass of a transform larger than one tile), so no
+// thread needs a bound check; without the checks the pass runs about 5% faster
+// (2^24 BN254-Fr, B200).
+template <class F, int LOG_TILE, int THREADS, bool COHERENT, bool EXT, bool FULL = false>
 __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uint4* sm) {
   constexpr uint32_t TILE_MAX = 1u << LOG_TILE;
   const uint32_t k = pp.k, c = pp.c, C = 1u << c;
-  const uint32_t tile = 1u << (k + c);
+  const uint32_t tile = FULL ? TILE_MAX : 1u << (k + c);
   const uint32_t tid = threadIdx.x;
 
   uint64_t hi_base = 0, m0 = 0, col0 = 0;
@@ -106,7 +109,7 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
 #pragma unroll
   for (uint32_t q = 0; q < 2 * TILE_MAX / THREADS; q++) {
     const uint32_t idx = tid + q * THREADS;
-    if (idx < 2 * tile) {
+    if (FULL || idx < 2 * tile) {
       const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
       uint64_t g;
       uint32_t t;
@@ -134,7 +137,7 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
 #pragma unroll
     for (uint32_t q = 0; q < TILE_MAX / 2 / THREADS; q++) {
       const uint32_t b = tid + q * THREADS;
-      if (b < tile / 2) {
+      if (FULL || b < tile / 2) {
         const uint32_t col = b & (C - 1), t0 = (b >> c) << 1;  // half = 1: j = 0
         const uint64_t jg = pp.first ? 0 : m0 + col;
         const uint32_t e0 = (t0 << c) | col, e1 = e0 + C;
@@ -161,7 +164,7 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
 #pragma unroll
     for (uint32_t q = 0; q < TILE_MAX / 4 / THREADS; q++) {
       const uint32_t ga = tid + q * THREADS;
-      if (ga < tile / 4) {
+      if (FULL || ga < tile / 4) {
         const uint32_t col = ga & (C - 1), g = ga >> c;
         const uint32_t j = g & (h - 1);
         const uint32_t t0 = ((g >> (i - 1)) << (i + 1)) | j;
@@ -206,7 +209,7 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
 #pragma unroll
     for (uint32_t q = 0; q < TILE_MAX / THREADS; q++) {
       const uint32_t e = tid + q * THREADS;
-      if (e < tile) {
+      if (FULL || e < tile) {
         const uint32_t col = e & (C - 1), row = e >> c;
         if (EXT && pp.scale_tab) {
           const uint64_t g = pp.first ? ((uint64_t)rev_bits((uint32_t)(col0 + col), xcols_log) << k) + row
@@ -222,7 +225,7 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
 #pragma unroll
   for (uint32_t q = 0; q < 2 * TILE_MAX / THREADS; q++) {
     const uint32_t idx = tid + q * THREADS;
-    if (idx < 2 * tile) {
+    if (FULL || idx < 2 * tile) {
       const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
       uint64_t g;
       if (pp.first) {

@@ -137,7 +137,8 @@ def replay(z, torch, F, trace, work: Workload, hbm_budget: int, serial: bool, sl
     last_done = [0]
 
     diag = {"pinned_allocs": 0, "pinned_alloc_ms": 0.0, "max_verify_ms": 0.0, "gc_pause_ms": 0.0,
-            "max_gc_pause_ms": 0.0}
+            "max_gc_pause_ms": 0.0, "pinned_alloc_events": []}
+    t_start = [time.perf_counter()]
 
     def out_buf(L):
         with lock:
@@ -146,8 +147,11 @@ def replay(z, torch, F, trace, work: Workload, hbm_budget: int, serial: bool, sl
                 return lst.pop()
         t = time.perf_counter()
         b = torch.empty((1 << L) * 4, dtype=torch.int64, pin_memory=True)
+        dt = 1e3 * (time.perf_counter() - t)
         diag["pinned_allocs"] += 1
-        diag["pinned_alloc_ms"] += 1e3 * (time.perf_counter() - t)
+        diag["pinned_alloc_ms"] += dt
+        if len(diag["pinned_alloc_events"]) < 16:
+            diag["pinned_alloc_events"].append((round(t - t_start[0], 4), L, round(dt, 3)))
         return b
 
     gc_t = [0.0]
@@ -223,11 +227,13 @@ def replay(z, torch, F, trace, work: Workload, hbm_budget: int, serial: bool, sl
         cap = 256 if L <= 14 else 64 if L <= 17 else 16
         pools[L] = [torch.empty((1 << L) * 4, dtype=torch.int64, pin_memory=True) for _ in range(min(c, cap))]
     th = threading.Thread(target=consume, daemon=True)
+    pool0 = z.pool_stats()
     gc.callbacks.append(gc_cb)
     old_switch = sys.getswitchinterval()
     sys.setswitchinterval(5e-5)  # hand the interpreter over quickly between submitter and consumer
     th.start()
     t0 = z.now_ns() + 20_000_000
+    t_start[0] = time.perf_counter() + 0.02
     late = 0
     for tag, (a, k, L, v) in enumerate(trace):
         arrival = t0 + int(a * 1e9)
@@ -250,6 +256,8 @@ def replay(z, torch, F, trace, work: Workload, hbm_budget: int, serial: bool, sl
     gc.callbacks.remove(gc_cb)
     stats = server.stats()
     server.close()
+    pool1 = z.pool_stats()
+    diag["pool_device_mallocs"] = pool1["device_mallocs"] - pool0["device_mallocs"]
     lat_a = np.array(lat)
     rec = np.array(records, dtype=np.float64)
     worst = rec[np.argsort(rec[:, 6] - rec[:, 3])[-8:]] if len(rec) else rec
