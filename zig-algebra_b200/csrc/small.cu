@@ -90,12 +90,14 @@ __device__ __forceinline__ void small_butterfly(uint64_t& u, uint64_t& v, bool m
 }
 
 // One tile of one pass.  PAD: the first pass reads natural indices at or
-// beyond pp.src_len as zeros (a zero-padded input that is not stored).
-template <class SF, int LOG_TILE, int THREADS, bool PAD>
+// beyond pp.src_len as zeros (a zero-padded input that is not stored).  FULL:
+// the tile is the whole 2^LOG_TILE (k + c == LOG_TILE), so no bound checks
+// (2^24 BabyBear about 10% faster without them on B200).
+template <class SF, int LOG_TILE, int THREADS, bool PAD, bool FULL = false>
 __device__ __forceinline__ void small_pass_body(const SmallPass& pp, uint32_t blk, uint64_t* sm) {
   constexpr uint32_t TILE_MAX = 1u << LOG_TILE;
   const uint32_t k = pp.k, c = pp.c, C = 1u << c;
-  const uint32_t tile = 1u << (k + c);
+  const uint32_t tile = FULL ? TILE_MAX : 1u << (k + c);
   const uint32_t tid = threadIdx.x;
   uint32_t hi_base = 0, m0 = 0, col0 = 0;
   if (pp.first) {
@@ -110,7 +112,7 @@ __device__ __forceinline__ void small_pass_body(const SmallPass& pp, uint32_t bl
 #pragma unroll
   for (uint32_t q = 0; q < TILE_MAX / THREADS; q++) {
     const uint32_t e = tid + q * THREADS;
-    if (e < tile) {
+    if (FULL || e < tile) {
       const uint32_t col = e & (C - 1), row = e >> c;
       uint32_t g, t;
       if (pp.first) {
@@ -132,7 +134,7 @@ __device__ __forceinline__ void small_pass_body(const SmallPass& pp, uint32_t bl
 #pragma unroll
     for (uint32_t q = 0; q < TILE_MAX / 2 / THREADS; q++) {
       const uint32_t b = tid + q * THREADS;
-      if (b < tile / 2) {
+      if (FULL || b < tile / 2) {
         const uint32_t col = b & (C - 1), t0 = (b >> c) << 1;
         const uint32_t jg = pp.first ? 0 : m0 + col;
         const uint32_t e0 = (t0 << c) | col, e1 = e0 + C;
@@ -154,7 +156,7 @@ __device__ __forceinline__ void small_pass_body(const SmallPass& pp, uint32_t bl
 #pragma unroll
     for (uint32_t q = 0; q < TILE_MAX / 4 / THREADS; q++) {
       const uint32_t ga = tid + q * THREADS;
-      if (ga < tile / 4) {
+      if (FULL || ga < tile / 4) {
         const uint32_t col = ga & (C - 1), g = ga >> c;
         const uint32_t j = g & (h - 1);
         const uint32_t t0 = ((g >> (i - 1)) << (i + 1)) | j;
@@ -188,7 +190,7 @@ __device__ __forceinline__ void small_pass_body(const SmallPass& pp, uint32_t bl
 #pragma unroll
   for (uint32_t q = 0; q < TILE_MAX / THREADS; q++) {
     const uint32_t e = tid + q * THREADS;
-    if (e < tile) {
+    if (FULL || e < tile) {
       const uint32_t col = e & (C - 1), row = e >> c;
       const uint32_t g = pp.first ? (rev_bits_small(col0 + col, xcols_log) << k) + row
                                   : hi_base + (row << pp.S) + m0 + col;
@@ -199,22 +201,22 @@ __device__ __forceinline__ void small_pass_body(const SmallPass& pp, uint32_t bl
   }
 }
 
-template <class SF, int LOG_TILE, int THREADS>
+template <class SF, int LOG_TILE, int THREADS, bool FULL>
 __global__ void __launch_bounds__(THREADS) small_pass_kernel(SmallPass pp) {
   __shared__ uint64_t sm[1u << LOG_TILE];
-  small_pass_body<SF, LOG_TILE, THREADS, false>(pp, blockIdx.x, sm);
+  small_pass_body<SF, LOG_TILE, THREADS, false, FULL>(pp, blockIdx.x, sm);
 }
 
 // The same pass over many columns of one size: column blockIdx.y reads
 // srcs[y] and writes dsts[y] (device pointer tables).
-template <class SF, int LOG_TILE, int THREADS>
+template <class SF, int LOG_TILE, int THREADS, bool FULL>
 __global__ void __launch_bounds__(THREADS) small_pass_cols_kernel(SmallPass pp, const uint64_t* const* srcs,
                                                                   uint64_t* const* dsts) {
   __shared__ uint64_t sm[1u << LOG_TILE];
   SmallPass q = pp;
   q.src = srcs[blockIdx.y];
   q.dst = dsts[blockIdx.y];
-  small_pass_body<SF, LOG_TILE, THREADS, true>(q, blockIdx.x, sm);
+  small_pass_body<SF, LOG_TILE, THREADS, true, FULL>(q, blockIdx.x, sm);
 }
 
 // Flat table entry e = 2^s - 1 + j holds root^(j * 2^(log_n - 1 - s)), in
@@ -312,21 +314,38 @@ __global__ void small_bit_reverse_kernel(const uint64_t* __restrict__ src, uint6
 
 int grid_for(uint64_t count) { return (int)std::min<uint64_t>((count + 255) / 256, 148 * 16); }
 
+template <class SF, bool FULL>
+static void launch_small_pass_t(const SmallPass& pp, uint64_t tiles, cudaStream_t st) {
+  small_pass_kernel<SF, kSmallLogTile, kSmallThreads, FULL><<<(unsigned)tiles, kSmallThreads, 0, st>>>(pp);
+}
+
 cudaError_t launch_small_pass(int field, const SmallPass& pp, uint64_t tiles, cudaStream_t st) {
-  if (field == kGoldilocksField)
-    small_pass_kernel<Goldilocks, kSmallLogTile, kSmallThreads><<<(unsigned)tiles, kSmallThreads, 0, st>>>(pp);
-  else
-    small_pass_kernel<BabyBear, kSmallLogTile, kSmallThreads><<<(unsigned)tiles, kSmallThreads, 0, st>>>(pp);
+  const bool full = pp.k + pp.c == (uint32_t)kSmallLogTile;
+  if (field == kGoldilocksField) {
+    if (full) launch_small_pass_t<Goldilocks, true>(pp, tiles, st);
+    else launch_small_pass_t<Goldilocks, false>(pp, tiles, st);
+  } else {
+    if (full) launch_small_pass_t<BabyBear, true>(pp, tiles, st);
+    else launch_small_pass_t<BabyBear, false>(pp, tiles, st);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t launch_small_pass_cols(int field, const SmallPass& pp, uint64_t tiles, uint32_t m,
                                    const uint64_t* const* srcs, uint64_t* const* dsts, cudaStream_t st) {
   const dim3 grid((unsigned)tiles, m);
-  if (field == kGoldilocksField)
-    small_pass_cols_kernel<Goldilocks, kSmallLogTile, kSmallThreads><<<grid, kSmallThreads, 0, st>>>(pp, srcs, dsts);
-  else
-    small_pass_cols_kernel<BabyBear, kSmallLogTile, kSmallThreads><<<grid, kSmallThreads, 0, st>>>(pp, srcs, dsts);
+  const bool full = pp.k + pp.c == (uint32_t)kSmallLogTile;
+  if (field == kGoldilocksField) {
+    if (full)
+      small_pass_cols_kernel<Goldilocks, kSmallLogTile, kSmallThreads, true><<<grid, kSmallThreads, 0, st>>>(pp, srcs, dsts);
+    else
+      small_pass_cols_kernel<Goldilocks, kSmallLogTile, kSmallThreads, false><<<grid, kSmallThreads, 0, st>>>(pp, srcs, dsts);
+  } else {
+    if (full)
+      small_pass_cols_kernel<BabyBear, kSmallLogTile, kSmallThreads, true><<<grid, kSmallThreads, 0, st>>>(pp, srcs, dsts);
+    else
+      small_pass_cols_kernel<BabyBear, kSmallLogTile, kSmallThreads, false><<<grid, kSmallThreads, 0, st>>>(pp, srcs, dsts);
+  }
   return cudaGetLastError();
 }
 
