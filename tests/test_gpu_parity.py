@@ -220,7 +220,8 @@ def test_lazy_reduction_bounds(z, log_n):
     [0, 2p) inside a pass and skips each product's final subtraction; with every element and
     every twiddle at p - 1 (raw limbs, so tw[s][0] != 1 and every butterfly multiplies) the sums
     and differences meet 2p - 2 and the products their largest inputs.  Also alternating 0 / p - 1
-    data, and p - 1 data against tables of 1 and of Montgomery one.  Under the default plan
+    data, and p - 1 data against tables of 1, of Montgomery one and of 0 (the inverse multiplies
+    by p - tw, which is p for a zero entry: still a valid factor).  Under the default plan
     (2^11-element tiles, at most 10 stages per pass) 2^10 and 2^11 run one pass, 2^16 two and
     2^21 three, so every pass boundary's reduction to [0, p) is crossed.  Both directions,
     nttWithTwiddles / inttWithTwiddles (libs/ntt/src/root.zig:148-212; the arithmetic is
@@ -240,7 +241,8 @@ def test_lazy_reduction_bounds(z, log_n):
         cases = [("p-1 data, p-1 table", filled(pm1, n), pm1),
                  ("alternating 0/p-1 data, p-1 table", alternating, pm1),
                  ("p-1 data, table of 1", filled(pm1, n), one),
-                 ("p-1 data, table of Montgomery one", filled(pm1, n), mont_one)]
+                 ("p-1 data, table of Montgomery one", filled(pm1, n), mont_one),
+                 ("p-1 data, table of 0", filled(pm1, n), zero)]
         for name, x, tv in cases:
             table = [filled(tv, 1 << s) for s in range(log_n)]
             for inverse in (False, True):

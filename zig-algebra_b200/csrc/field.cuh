@@ -204,6 +204,29 @@ __device__ __forceinline__ fe fe_neg(const fe& a) {
   return fe_sub<F>(z, a);
 }
 
+// p - a for a in [0, p]: the negation of a twiddle factor as a multiplier.  For
+// a != 0 it is -a mod p; for a = 0 it is p, which is not canonical but is a
+// valid left operand of fe_mul (the CIOS bound needs a <= p: the running value
+// stays below 2p) and gives the same reduced product as 0.  One subtraction
+// chain, no select: cheaper than fe_neg on the inverse transform's hot path.
+template <class F>
+__device__ __forceinline__ fe fe_p_minus(const fe& a) {
+  fe r;
+  asm("sub.cc.u32  %0, %8, %16;\n\t"
+      "subc.cc.u32 %1, %9, %17;\n\t"
+      "subc.cc.u32 %2, %10, %18;\n\t"
+      "subc.cc.u32 %3, %11, %19;\n\t"
+      "subc.cc.u32 %4, %12, %20;\n\t"
+      "subc.cc.u32 %5, %13, %21;\n\t"
+      "subc.cc.u32 %6, %14, %22;\n\t"
+      "subc.u32    %7, %15, %23;"
+      : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]), "=r"(r.v[6]),
+        "=r"(r.v[7])
+      : "n"(F::P0), "n"(F::P1), "n"(F::P2), "n"(F::P3), "n"(F::P4), "n"(F::P5), "n"(F::P6), "n"(F::P7),
+        "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]));
+  return r;
+}
+
 // x in [0, 2p) -> [0, p): one conditional subtraction of p.
 template <class F>
 __device__ __forceinline__ fe fe_reduce(const fe& x) {

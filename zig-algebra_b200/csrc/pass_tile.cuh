@@ -35,7 +35,8 @@ __device__ __forceinline__ void sm_store(uint4* sm, uint32_t e, const fe& a) {
 // Twiddle of global stage s (1-based) for butterfly index jg, with the
 // forward (tw[s-1][jg]) or inttWithTwiddles (1 or -tw[s-1][2^(s-1) - jg])
 // mapping.  `stw` points at tw[s-1]; returns false when the factor is one and
-// the multiply can be skipped.
+// the multiply can be skipped.  The inverse's factor is p - tw (fe_p_minus):
+// the product equals the one by -tw mod p, also for a zero entry.
 template <class F>
 __device__ __forceinline__ bool twiddle(const PassParams& pp, const uint4* stw, uint64_t half_g, uint64_t jg,
                                         fe& w) {
@@ -43,7 +44,7 @@ __device__ __forceinline__ bool twiddle(const PassParams& pp, const uint4* stw, 
   if (!pp.inverse) {
     w = fe_load_nc(stw + (jg << 1));
   } else {
-    w = fe_neg<F>(fe_load_nc(stw + ((half_g - jg) << 1)));
+    w = fe_p_minus<F>(fe_load_nc(stw + ((half_g - jg) << 1)));
   }
   return true;
 }
