@@ -62,6 +62,32 @@ cudaError_t BufferPool::acquire(size_t bytes, void** out) {
     cached_ -= bytes;
     return cudaSuccess;
   }
+  if (bytes <= kSlabMax) {
+    const size_t need = (bytes + 255) & ~(size_t)255;  // 256-byte aligned pieces
+    if (slabs_.empty() || slab_used_ + need > slabs_.back().second) {
+      void* slab = nullptr;
+      mallocs_++;
+      cudaError_t e = cudaMalloc(&slab, kSlabBytes);
+      if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        trim();
+        mallocs_++;
+        e = cudaMalloc(&slab, kSlabBytes);
+      }
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        slab = nullptr;
+      } else {
+        slabs_.push_back({static_cast<char*>(slab), kSlabBytes});
+        slab_used_ = 0;
+      }
+    }
+    if (!slabs_.empty() && slab_used_ + need <= slabs_.back().second) {
+      *out = slabs_.back().first + slab_used_;
+      slab_used_ += need;
+      return cudaSuccess;
+    }
+  }
   mallocs_++;
   cudaError_t e = cudaMalloc(out, bytes);
   if (e == cudaErrorMemoryAllocation) {
@@ -73,6 +99,13 @@ cudaError_t BufferPool::acquire(size_t bytes, void** out) {
   return e;
 }
 
+bool BufferPool::in_slab(const void* p) const {
+  const char* c = static_cast<const char*>(p);
+  for (const auto& s : slabs_)
+    if (c >= s.first && c < s.first + s.second) return true;
+  return false;
+}
+
 void BufferPool::release(void* p, size_t bytes) {
   if (!p) return;
   free_.emplace(bytes, p);
@@ -80,8 +113,24 @@ void BufferPool::release(void* p, size_t bytes) {
 }
 
 void BufferPool::trim() {
-  for (auto& kv : free_) cudaFree(kv.second);
+  for (auto it = free_.begin(); it != free_.end();) {
+    if (in_slab(it->second)) {
+      ++it;
+      continue;
+    }
+    cudaFree(it->second);
+    cached_ -= it->first;
+    it = free_.erase(it);
+  }
+}
+
+void BufferPool::release_all() {
+  for (auto& kv : free_)
+    if (!in_slab(kv.second)) cudaFree(kv.second);
   free_.clear();
+  for (auto& s : slabs_) cudaFree(s.first);
+  slabs_.clear();
+  slab_used_ = 0;
   cached_ = 0;
 }
 
@@ -554,7 +603,7 @@ int zntt_shutdown(void) {
   fri_shutdown();
   free_coset_tabs();
   c.regs.clear();
-  c.pool.trim();
+  c.pool.release_all();
   for (cudaStream_t& p : c.pipe)
     if (p) {
       cudaStreamDestroy(p);

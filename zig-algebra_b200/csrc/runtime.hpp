@@ -65,17 +65,29 @@ struct TuneEntry {
 };
 
 // Caching device allocator: freed buffers are kept by exact size for reuse.
+// Buffers of at most kSlabMax bytes are carved from kSlabBytes slabs, so a
+// burst of small requests (the server's transforms of 2^10..2^15 elements)
+// costs one cudaMalloc per slab, not one per buffer: a cudaMalloc issued while
+// batches run can stall the host thread that issues it for a long time.
 class BufferPool {
  public:
+  static constexpr size_t kSlabMax = (size_t)1 << 20;
+  static constexpr size_t kSlabBytes = (size_t)64 << 20;
   cudaError_t acquire(size_t bytes, void** out);
   void release(void* p, size_t bytes);
+  // Frees the idle buffers that own their memory (slab pieces stay cached).
   void trim();
+  // Frees everything, slabs included; no buffer may be in use.
+  void release_all();
   size_t cached_bytes() const { return cached_; }
   uint64_t acquires() const { return acquires_; }
   uint64_t device_mallocs() const { return mallocs_; }
 
  private:
+  bool in_slab(const void* p) const;
   std::multimap<size_t, void*> free_;
+  std::vector<std::pair<char*, size_t>> slabs_;
+  size_t slab_used_ = 0;  // bytes carved from the last slab
   size_t cached_ = 0;
   uint64_t acquires_ = 0;  // acquire() calls
   uint64_t mallocs_ = 0;   // cudaMalloc calls made by acquire()

@@ -223,8 +223,10 @@ def replay(z, torch, F, trace, work: Workload, hbm_budget: int, serial: bool, sl
     counts: dict[int, int] = {}
     for _, _, L, _ in trace:
         counts[L] = counts.get(L, 0) + 1
+    # Up to 256 MB per size (at least 16 buffers): a pinned allocation during the replay
+    # stalls the submitting thread for milliseconds to hundreds of milliseconds.
     for L, c in counts.items():
-        cap = 256 if L <= 14 else 64 if L <= 17 else 16
+        cap = max(16, (256 << 20) // (32 << L))
         pools[L] = [torch.empty((1 << L) * 4, dtype=torch.int64, pin_memory=True) for _ in range(min(c, cap))]
     th = threading.Thread(target=consume, daemon=True)
     pool0 = z.pool_stats()
