@@ -35,7 +35,9 @@ __device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
   return v;
 }
 
-template <class F, int LOG_TILE, int THREADS, int MINB, bool EXT>
+// FULL: every pass of the batch has whole tiles (k + c == LOG_TILE), so the
+// tile runs without bound checks, as the plain pass kernel does for such passes.
+template <class F, int LOG_TILE, int THREADS, int MINB, bool EXT, bool FULL>
 __global__ void __launch_bounds__(THREADS, MINB)
     batch_kernel(const BatchPass* __restrict__ passes, const BatchItem* __restrict__ items, uint32_t n_items,
                  uint32_t* ctl, uint32_t spin_limit) {
@@ -77,31 +79,37 @@ __global__ void __launch_bounds__(THREADS, MINB)
     const uint32_t* src = reinterpret_cast<const uint32_t*>(&passes[item.pass].pp);
     for (int w = threadIdx.x; w < kWords; w += THREADS) reinterpret_cast<uint32_t*>(&s_pp)[w] = src[w];
     __syncthreads();
-    ntt_tile<F, LOG_TILE, THREADS, true, EXT>(s_pp, item.tile, sm);
+    ntt_tile<F, LOG_TILE, THREADS, true, EXT, FULL>(s_pp, item.tile, sm);
     __threadfence();  // this thread's stores are visible device-wide ...
     __syncthreads();  // ... for every thread of the CTA, before the count
     if (threadIdx.x == 0) atomicAdd(&ctl[2 + item.pass], 1u);
   }
 }
 
-template <class F, int SH, bool EXT>
+template <class F, int SH, bool EXT, bool FULL>
 static void* batch_ptr() {
-  return (void*)batch_kernel<F, kShapes[SH].log_tile, kShapes[SH].threads, kShapes[SH].min_blocks, EXT>;
+  return (void*)batch_kernel<F, kShapes[SH].log_tile, kShapes[SH].threads, kShapes[SH].min_blocks, EXT, FULL>;
+}
+
+template <class F, int SH>
+static void* batch_shape_ptr(bool ext, bool full) {
+  if (ext) return full ? batch_ptr<F, SH, true, true>() : batch_ptr<F, SH, true, false>();
+  return full ? batch_ptr<F, SH, false, true>() : batch_ptr<F, SH, false, false>();
 }
 
 template <class F>
-static void* batch_kernel_ptr(int shape, bool ext) {
-  if (shape == 0) return ext ? batch_ptr<F, 0, true>() : batch_ptr<F, 0, false>();
-  return ext ? batch_ptr<F, 1, true>() : batch_ptr<F, 1, false>();
+static void* batch_kernel_ptr(int shape, bool ext, bool full) {
+  return shape == 0 ? batch_shape_ptr<F, 0>(ext, full) : batch_shape_ptr<F, 1>(ext, full);
 }
 
 cudaError_t configure_batch_kernels() {
   for (int sh = 0; sh < kNumShapes; sh++) {
-    for (int ext = 0; ext < 2; ext++) {
-      cudaError_t e = cudaFuncSetAttribute(batch_kernel_ptr<Bn254Fr>(sh, ext), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           shape_smem_bytes(sh));
+    for (int v = 0; v < 4; v++) {
+      const bool ext = v & 1, full = v & 2;
+      cudaError_t e = cudaFuncSetAttribute(batch_kernel_ptr<Bn254Fr>(sh, ext, full),
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, shape_smem_bytes(sh));
       if (e != cudaSuccess) return e;
-      e = cudaFuncSetAttribute(batch_kernel_ptr<Bls12381Fr>(sh, ext), cudaFuncAttributeMaxDynamicSharedMemorySize,
+      e = cudaFuncSetAttribute(batch_kernel_ptr<Bls12381Fr>(sh, ext, full), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                shape_smem_bytes(sh));
       if (e != cudaSuccess) return e;
     }
@@ -113,38 +121,45 @@ int batch_grid(int field, int shape, bool ext) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  void* fn = field == kBn254Fr ? batch_kernel_ptr<Bn254Fr>(shape, ext) : batch_kernel_ptr<Bls12381Fr>(shape, ext);
+  void* fn = field == kBn254Fr ? batch_kernel_ptr<Bn254Fr>(shape, ext, false) : batch_kernel_ptr<Bls12381Fr>(shape, ext, false);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kShapes[shape].threads, shape_smem_bytes(shape));
   if (per_sm < 1) per_sm = 1;
   return sms * per_sm;
 }
 
-template <class F, int SH, bool EXT>
+template <class F, int SH, bool EXT, bool FULL>
 static void launch_batch_k(const BatchPass* passes, const BatchItem* items, uint32_t n_items, uint32_t* ctl,
                            uint32_t spin_limit, int grid, cudaStream_t st) {
   constexpr PassShape S = kShapes[SH];
-  batch_kernel<F, S.log_tile, S.threads, S.min_blocks, EXT>
+  batch_kernel<F, S.log_tile, S.threads, S.min_blocks, EXT, FULL>
       <<<grid, S.threads, shape_smem_bytes(SH), st>>>(passes, items, n_items, ctl, spin_limit);
 }
 
-template <class F>
-static void launch_batch_typed(int shape, bool ext, const BatchPass* passes, const BatchItem* items, uint32_t n_items,
+template <class F, int SH>
+static void launch_batch_shape(bool ext, bool full, const BatchPass* passes, const BatchItem* items, uint32_t n_items,
                                uint32_t* ctl, uint32_t spin_limit, int grid, cudaStream_t st) {
-  if (shape == 0) {
-    if (ext) launch_batch_k<F, 0, true>(passes, items, n_items, ctl, spin_limit, grid, st);
-    else launch_batch_k<F, 0, false>(passes, items, n_items, ctl, spin_limit, grid, st);
+  if (ext) {
+    if (full) launch_batch_k<F, SH, true, true>(passes, items, n_items, ctl, spin_limit, grid, st);
+    else launch_batch_k<F, SH, true, false>(passes, items, n_items, ctl, spin_limit, grid, st);
   } else {
-    if (ext) launch_batch_k<F, 1, true>(passes, items, n_items, ctl, spin_limit, grid, st);
-    else launch_batch_k<F, 1, false>(passes, items, n_items, ctl, spin_limit, grid, st);
+    if (full) launch_batch_k<F, SH, false, true>(passes, items, n_items, ctl, spin_limit, grid, st);
+    else launch_batch_k<F, SH, false, false>(passes, items, n_items, ctl, spin_limit, grid, st);
   }
 }
 
-cudaError_t launch_batch(int field, int shape, bool ext, const BatchPass* passes, const BatchItem* items,
+template <class F>
+static void launch_batch_typed(int shape, bool ext, bool full, const BatchPass* passes, const BatchItem* items,
+                               uint32_t n_items, uint32_t* ctl, uint32_t spin_limit, int grid, cudaStream_t st) {
+  if (shape == 0) launch_batch_shape<F, 0>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st);
+  else launch_batch_shape<F, 1>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st);
+}
+
+cudaError_t launch_batch(int field, int shape, bool ext, bool full, const BatchPass* passes, const BatchItem* items,
                          uint32_t n_items, uint32_t* ctl, uint32_t spin_limit, int grid, cudaStream_t st) {
   if (field == kBn254Fr)
-    launch_batch_typed<Bn254Fr>(shape, ext, passes, items, n_items, ctl, spin_limit, grid, st);
+    launch_batch_typed<Bn254Fr>(shape, ext, full, passes, items, n_items, ctl, spin_limit, grid, st);
   else
-    launch_batch_typed<Bls12381Fr>(shape, ext, passes, items, n_items, ctl, spin_limit, grid, st);
+    launch_batch_typed<Bls12381Fr>(shape, ext, full, passes, items, n_items, ctl, spin_limit, grid, st);
   return cudaGetLastError();
 }
 

@@ -169,7 +169,8 @@ struct zntt_batch {
   uint32_t* d_ctl = nullptr;
   size_t ctl_words = 0;
   int grid = 0;
-  bool ext = false;  // some pass pads or scales by a table
+  bool ext = false;   // some pass pads or scales by a table
+  bool full = false;  // every pass has whole tiles (the kernel runs without bound checks)
   uint32_t spin_limit = ZNTT_BATCH_SPIN_LIMIT;  // x ~0.25-1 us: a stalled dependency gives up after seconds
   std::vector<std::pair<void*, size_t>> scratch;  // pool buffers owned by the batch
   std::vector<CosetTab*> coset_tabs;
@@ -340,6 +341,7 @@ int zntt_batch_create(int field, const zntt_job* jobs, size_t n_jobs, int shape,
     return cuda_fail(ce, "batch set-up");
   }
   for (const BatchPass& bp : b->passes) b->ext = b->ext || pass_needs_ext(bp.pp);
+  b->full = !b->passes.empty() && batch_all_full(b->shape, b->passes.data(), b->passes.size());
   b->grid = std::max(1, std::min<int>(batch_grid(field, b->shape, b->ext), (int)std::max<size_t>(1, b->items.size())));
   *out = b;
   return ZNTT_OK;
@@ -349,7 +351,7 @@ static int enqueue_batch(zntt_batch* b, cudaStream_t st) {
   cudaError_t ce = cudaMemsetAsync(b->d_ctl, 0, b->ctl_words * 4, st);
   if (ce != cudaSuccess) return cuda_fail(ce, "batch reset");
   if (b->items.empty()) return ZNTT_OK;
-  ce = launch_batch(b->field, b->shape, b->ext, b->d_passes, b->d_items, (uint32_t)b->items.size(), b->d_ctl,
+  ce = launch_batch(b->field, b->shape, b->ext, b->full, b->d_passes, b->d_items, (uint32_t)b->items.size(), b->d_ctl,
                     b->spin_limit, b->grid, st);
   if (ce != cudaSuccess) return cuda_fail(ce, "batch launch");
   return ZNTT_OK;

@@ -80,8 +80,15 @@ struct BatchItem {
 // ctl[0]: next item, ctl[1]: error flag, ctl[2 + p]: finished tiles of pass p.
 // Every wait for a finished pass spins at most `spin_limit` rounds of ~1 us,
 // then raises the error flag; every CTA stops at the next item once it is set.
-cudaError_t launch_batch(int field, int shape, bool ext, const BatchPass* passes, const BatchItem* items,
+// `full`: every pass has whole tiles (batch_all_full), so no bound checks.
+cudaError_t launch_batch(int field, int shape, bool ext, bool full, const BatchPass* passes, const BatchItem* items,
                          uint32_t n_items, uint32_t* ctl, uint32_t spin_limit, int grid, cudaStream_t st);
+// True when every pass's tile is the shape's whole tile (k + c == log_tile).
+inline bool batch_all_full(int shape, const BatchPass* passes, size_t n) {
+  for (size_t i = 0; i < n; i++)
+    if (passes[i].pp.k + passes[i].pp.c != (uint32_t)kShapes[shape].log_tile) return false;
+  return true;
+}
 int batch_grid(int field, int shape, bool ext);
 
 // Flat zig-ntt twiddle table for one (field, log_n, root): entry 2^s - 1 + j

@@ -325,7 +325,9 @@ static bool launch_into(zntt_server* s, Slot& sl) {
     if (ce == cudaSuccess) ce = cudaMemsetAsync(sl.d_ctl, 0, (2 + np) * 4, st);
     if (ce == cudaSuccess) {
       const int grid = std::max(1, std::min<int>(ext ? s->grid_ext : s->grid_plain, (int)ni));
-      ce = launch_batch(field, kDefaultShape, ext, sl.d_passes, sl.d_items, ni, sl.d_ctl, 4u << 20, grid, st);
+      const bool full = batch_all_full(kDefaultShape, sl.h_passes, np);
+      ce = launch_batch(field, kDefaultShape, ext, full, sl.d_passes, sl.d_items, ni, sl.d_ctl, ZNTT_BATCH_SPIN_LIMIT,
+                        grid, st);
     }
     if (ce == cudaSuccess) ce = cudaMemcpyAsync(sl.h_flag, sl.d_ctl + 1, 4, cudaMemcpyDeviceToHost, st);
   }
