@@ -363,10 +363,13 @@ int zntt_fri_query_extract(int field, uint32_t log_domain, uint32_t rounds, cons
  * admitted into one batch (one persistent launch) whenever one of `slots`
  * streams is free -- so new arrivals overlap on the device with batches
  * already running -- and posts completions with CLOCK_MONOTONIC timestamps.
- * Twiddle tables of every size served stay resident; device buffers return to
- * the pool after each request and are reused.  `serial` runs one request at
- * a time with plain per-pass launches (the baseline batching is measured
- * against). */
+ * Twiddle tables of every size served stay resident.  The server reserves
+ * min(hbm_budget_bytes, 8 GiB) of device memory when it is created and carves
+ * request buffers from it, reusing freed ones by size, so steady serving makes
+ * no cudaMalloc (one issued while batches run can stall the worker for
+ * hundreds of milliseconds); past that reserve, buffers come from the
+ * library's pool.  `serial` runs one request at a time with plain per-pass
+ * launches (the baseline batching is measured against). */
 typedef struct zntt_server_config {
   int field;
   size_t hbm_budget_bytes;  /* device bytes for request buffers (inputs, outputs, scratch) */

@@ -25,6 +25,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -85,6 +86,14 @@ struct zntt_server {
   zntt_server_stats stats;
   size_t cap_passes = 0, cap_items = 0;
   int grid_plain = 0, grid_ext = 0;
+  // Request buffers come from one device arena reserved at creation: freed
+  // buffers are reused by exact size, new ones are carved from the unused end,
+  // and only when the arena is spent does a buffer come from the pool.  A
+  // cudaMalloc issued while batches run stalled the worker for hundreds of
+  // milliseconds on B200, so steady serving makes none.
+  char* arena = nullptr;
+  size_t arena_bytes = 0, arena_used = 0;
+  std::multimap<size_t, void*> arena_free;
 };
 
 namespace zntt {
@@ -140,10 +149,36 @@ static void post(zntt_server* s, const SrvReq& q, int status, uint64_t t) {
   s->stats.completed++;
 }
 
+constexpr size_t kArenaMax = (size_t)8 << 30;
+
+// A request buffer of `bytes` (worker thread only).
+static int srv_get(zntt_server* s, size_t bytes, void** out) {
+  auto it = s->arena_free.find(bytes);
+  if (it != s->arena_free.end()) {
+    *out = it->second;
+    s->arena_free.erase(it);
+    return ZNTT_OK;
+  }
+  const size_t need = (bytes + 255) & ~(size_t)255;
+  if (s->arena && s->arena_used + need <= s->arena_bytes) {
+    *out = s->arena + s->arena_used;
+    s->arena_used += need;
+    return ZNTT_OK;
+  }
+  return pool_get(bytes, out);
+}
+
+static void srv_put(zntt_server* s, void* p, size_t bytes) {
+  if (!p) return;
+  const char* c = static_cast<const char*>(p);
+  if (s->arena && c >= s->arena && c < s->arena + s->arena_bytes) s->arena_free.emplace(bytes, p);
+  else pool_put(p, bytes);
+}
+
 static void release_req(zntt_server* s, SrvReq& q) {
-  if (q.d_in) pool_put(q.d_in, q.in_bytes);
-  if (q.d_out) pool_put(q.d_out, q.out_bytes);
-  if (q.d_coef) pool_put(q.d_coef, q.coef_bytes);
+  srv_put(s, q.d_in, q.in_bytes);
+  srv_put(s, q.d_out, q.out_bytes);
+  srv_put(s, q.d_coef, q.coef_bytes);
   if (q.ct) release_coset_tab(q.ct);
   const size_t b = q.in_bytes + q.out_bytes + q.coef_bytes;
   s->budget_left += b;
@@ -246,9 +281,9 @@ static bool launch_into(zntt_server* s, Slot& sl) {
   for (size_t j = 0; j < sl.reqs.size(); j++) {
     SrvReq& q = sl.reqs[j];
     const zntt_request& r = q.r;
-    int rc = pool_get(q.in_bytes, &q.d_in);
-    if (!rc) rc = pool_get(q.out_bytes, &q.d_out);
-    if (!rc && q.coef_bytes) rc = pool_get(q.coef_bytes, &q.d_coef);
+    int rc = srv_get(s, q.in_bytes, &q.d_in);
+    if (!rc) rc = srv_get(s, q.out_bytes, &q.d_out);
+    if (!rc && q.coef_bytes) rc = srv_get(s, q.coef_bytes, &q.d_coef);
     TwEntry* tw = nullptr;
     if (!rc) rc = table_for(s, r.log_n, &tw);
     if (rc) {
@@ -438,6 +473,10 @@ int zntt_server_create(const zntt_server_config* cfg, zntt_server** out) {
     if (ce == cudaSuccess) ce = cudaMalloc((void**)&sl.d_items, s->cap_items * sizeof(BatchItem));
     if (ce == cudaSuccess) ce = cudaMalloc((void**)&sl.d_ctl, (2 + s->cap_passes) * 4);
   }
+  if (ce == cudaSuccess) {
+    s->arena_bytes = std::min(s->cfg.hbm_budget_bytes, kArenaMax) & ~(size_t)255;
+    if (s->arena_bytes) ce = cudaMalloc((void**)&s->arena, s->arena_bytes);
+  }
   if (ce != cudaSuccess) {
     destroy_slots(s);
     delete s;
@@ -502,6 +541,7 @@ int zntt_server_destroy(zntt_server* s) {
   {
     std::lock_guard<std::recursive_mutex> lock(ctx().mu);
     destroy_slots(s);
+    if (s->arena) cudaFree(s->arena);
     for (TwEntry*& t : s->tables)
       if (t) {
         release_table(t);
