@@ -640,7 +640,7 @@ def run_batched_config(z, torch, stream, steps, warmup, seed=33):
     }
 
 
-def run_lde_config(z, torch, stream, steps, warmup, seed=44):
+def run_lde_config(z, torch, stream, steps, warmup, seed=44, jobs=64):
     """64 BLS12-381-Fr coset extensions 2^18 -> 2^20 (inverse, zero-pad, g^i with
     g = 5, forward): one persistent launch against plain per-polynomial passes."""
     F = z.BLS12_381_FR
@@ -648,9 +648,9 @@ def run_lde_config(z, torch, stream, steps, warmup, seed=44):
     tabs = TableCache(z, F)
     sptr = stream.cuda_stream
     evs, outs, pls, jobs = [], [], [], []
-    pool = torch.empty(64 * (1 << 18) * 4, dtype=torch.int64, device="cuda")
-    z.random_elements(F, seed, pool.data_ptr(), 64 << 18, stream=sptr)
-    for i in range(64):
+    pool = torch.empty(jobs * (1 << 18) * 4, dtype=torch.int64, device="cuda")
+    z.random_elements(F, seed, pool.data_ptr(), jobs << 18, stream=sptr)
+    for i in range(jobs):
         ev = pool[i * (1 << 18) * 4:(i + 1) * (1 << 18) * 4]
         out = torch.empty((1 << 20) * 4, dtype=torch.int64, device="cuda")
         pl = torch.empty_like(out)
@@ -672,10 +672,10 @@ def run_lde_config(z, torch, stream, steps, warmup, seed=44):
         b.status()
     exact = all(torch.equal(o, p) for o, p in zip(outs, pls))
     tabs.close()
-    modmuls = 64 * ((1 << 17) * 18 + (1 << 18) + (1 << 19) * 20)
+    modmuls = jobs * ((1 << 17) * 18 + (1 << 18) + (1 << 19) * 20)
     return {
-        "workload": "64 x coset LDE 2^18 -> 2^20 BLS12-381-Fr (g = 5), one persistent launch (CUDA graph)",
-        "ms_per_batch": ms_b / steps, "value": 64 * (1 << 20) * steps / (ms_b * 1e-3), "unit": "output elements/s",
+        "workload": f"{jobs} x coset LDE 2^18 -> 2^20 BLS12-381-Fr (g = 5), one persistent launch (CUDA graph)",
+        "ms_per_batch": ms_b / steps, "value": jobs * (1 << 20) * steps / (ms_b * 1e-3), "unit": "output elements/s",
         "plain_ms_per_batch": ms_p / steps, "speedup_vs_plain": ms_p / ms_b,
         "modmul_per_s": modmuls * steps / (ms_b * 1e-3), "bit_exact_vs_plain": exact,
     }
@@ -1078,8 +1078,8 @@ def run_single_config(args):
                                 cpu_sample=not args.no_cpu_baseline)
             metric = "BN254-Fr polynomial product coefficients/s (2^23 x 2^23 coefficients)"
         else:
-            r = run_lde_config(z, torch, stream, steps=args.steps, warmup=args.warmup)
-            metric = "batched coset LDE output elems/s (64 x 2^18 -> 2^20, BLS12-381-Fr)"
+            r = run_lde_config(z, torch, stream, steps=args.steps, warmup=args.warmup, jobs=args.lde_jobs)
+            metric = f"batched coset LDE output elems/s ({args.lde_jobs} x 2^18 -> 2^20, BLS12-381-Fr)"
     line = {"metric": metric, "value": r["value"], "unit": r["unit"], "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "data": "synthetic: seeded inputs",
             "config": {"workload": r["workload"]}, "detail": r}
@@ -1099,6 +1099,7 @@ def main():
                     help="skip the batched, coset-extension, polynomial-product, small-field and FRI lines")
     ap.add_argument("--workload", default="ntt", choices=["ntt", "serve", "batched", "lde", "poly", "small", "fri"])
     ap.add_argument("--no-serve", action="store_true", help="leave the serving trace out of the default run")
+    ap.add_argument("--lde-jobs", type=int, default=64, help="extensions in the --workload lde batch (profiling)")
     ap.add_argument("--serve-requests", type=int, default=20000)
     ap.add_argument("--serve-sweep", type=float, nargs="*", default=[8000.0, 32000.0])
     ap.add_argument("--serve-sweep-requests", type=int, default=6000)
