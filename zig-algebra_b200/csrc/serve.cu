@@ -278,6 +278,10 @@ static bool launch_into(zntt_server* s, Slot& sl) {
   std::lock_guard<std::recursive_mutex> lock(ctx().mu);
   std::vector<JobPlan> plans(sl.reqs.size());
   const int shape = kDefaultShape;
+  // One request alone runs as plain per-pass launches: the persistent launch
+  // pays off only when several requests share it (its queue upload and launch
+  // cost a lone small request about 60 us of latency).
+  const bool plain = s->cfg.serial || sl.reqs.size() == 1;
   for (size_t j = 0; j < sl.reqs.size(); j++) {
     SrvReq& q = sl.reqs[j];
     const zntt_request& r = q.r;
@@ -294,7 +298,7 @@ static bool launch_into(zntt_server* s, Slot& sl) {
       const bool inv = r.mode == ZNTT_INVERSE;
       uint64_t ninv[4];
       if (inv) n_inverse(field, r.log_n, ninv);
-      const Plan plan = s->cfg.serial ? tuned_plan(field, r.log_n) : batch_plan(field, r.log_n, shape);
+      const Plan plan = batch_plan(field, r.log_n, shape);
       plan_transform(plans[j], tw, plan, r.log_n, (const uint4*)q.d_in, (uint4*)q.d_out, (uint4*)q.d_out, inv,
                      inv ? ninv : nullptr, nullptr, 1ull << r.log_n, 1ull << r.log_n);
     } else {
@@ -305,8 +309,8 @@ static bool launch_into(zntt_server* s, Slot& sl) {
         fail_slot(s, sl, rc);
         return true;
       }
-      const Plan pi = s->cfg.serial ? tuned_plan(field, r.log_in) : batch_plan(field, r.log_in, shape);
-      const Plan po = s->cfg.serial ? tuned_plan(field, r.log_n) : batch_plan(field, r.log_n, shape);
+      const Plan pi = batch_plan(field, r.log_in, shape);
+      const Plan po = batch_plan(field, r.log_n, shape);
       plan_transform(plans[j], twi, pi, r.log_in, (const uint4*)q.d_in, (uint4*)q.d_coef, (uint4*)q.d_coef, true,
                      nullptr, q.ct->d, 1ull << r.log_in, 1ull << r.log_in);
       plan_transform(plans[j], tw, po, r.log_n, (const uint4*)q.d_coef, (uint4*)q.d_out, (uint4*)q.d_out, false,
@@ -319,12 +323,11 @@ static bool launch_into(zntt_server* s, Slot& sl) {
   for (size_t j = 0; j < sl.reqs.size() && ce == cudaSuccess; j++)
     ce = cudaMemcpyAsync(sl.reqs[j].d_in, sl.reqs[j].r.h_in, sl.reqs[j].in_bytes, cudaMemcpyHostToDevice, st);
   *sl.h_flag = 0;
-  if (s->cfg.serial) {
-    // Plain launches, one pass after another (the length-1 case is a copy).
+  if (plain) {
+    // Plain launches, one pass after another, with the same plans as the batch
+    // kernel's (a length-1 transform is one pass of no stage).
     for (size_t p = 0; p < plans[0].passes.size() && ce == cudaSuccess; p++)
-      ce = launch_ntt_pass(field, kDefaultShape, plans[0].passes[p], plans[0].tiles[p], st);
-    if (ce == cudaSuccess && plans[0].passes.empty())
-      ce = cudaMemcpyAsync(sl.reqs[0].d_out, sl.reqs[0].d_in, 32, cudaMemcpyDeviceToDevice, st);
+      ce = launch_ntt_pass(field, shape, plans[0].passes[p], plans[0].tiles[p], st);
   } else {
     // One persistent launch over every pass of every request, queued level by level.
     std::vector<uint32_t> first(plans.size());
