@@ -640,7 +640,7 @@ def run_batched_config(z, torch, stream, steps, warmup, seed=33):
     }
 
 
-def run_lde_config(z, torch, stream, steps, warmup, seed=44, jobs=64):
+def run_lde_config(z, torch, stream, steps, warmup, seed=44, count=64):
     """64 BLS12-381-Fr coset extensions 2^18 -> 2^20 (inverse, zero-pad, g^i with
     g = 5, forward): one persistent launch against plain per-polynomial passes."""
     F = z.BLS12_381_FR
@@ -648,9 +648,9 @@ def run_lde_config(z, torch, stream, steps, warmup, seed=44, jobs=64):
     tabs = TableCache(z, F)
     sptr = stream.cuda_stream
     evs, outs, pls, jobs = [], [], [], []
-    pool = torch.empty(jobs * (1 << 18) * 4, dtype=torch.int64, device="cuda")
-    z.random_elements(F, seed, pool.data_ptr(), jobs << 18, stream=sptr)
-    for i in range(jobs):
+    pool = torch.empty(count * (1 << 18) * 4, dtype=torch.int64, device="cuda")
+    z.random_elements(F, seed, pool.data_ptr(), count << 18, stream=sptr)
+    for i in range(count):
         ev = pool[i * (1 << 18) * 4:(i + 1) * (1 << 18) * 4]
         out = torch.empty((1 << 20) * 4, dtype=torch.int64, device="cuda")
         pl = torch.empty_like(out)
@@ -672,10 +672,10 @@ def run_lde_config(z, torch, stream, steps, warmup, seed=44, jobs=64):
         b.status()
     exact = all(torch.equal(o, p) for o, p in zip(outs, pls))
     tabs.close()
-    modmuls = jobs * ((1 << 17) * 18 + (1 << 18) + (1 << 19) * 20)
+    modmuls = count * ((1 << 17) * 18 + (1 << 18) + (1 << 19) * 20)
     return {
-        "workload": f"{jobs} x coset LDE 2^18 -> 2^20 BLS12-381-Fr (g = 5), one persistent launch (CUDA graph)",
-        "ms_per_batch": ms_b / steps, "value": jobs * (1 << 20) * steps / (ms_b * 1e-3), "unit": "output elements/s",
+        "workload": f"{count} x coset LDE 2^18 -> 2^20 BLS12-381-Fr (g = 5), one persistent launch (CUDA graph)",
+        "ms_per_batch": ms_b / steps, "value": count * (1 << 20) * steps / (ms_b * 1e-3), "unit": "output elements/s",
         "plain_ms_per_batch": ms_p / steps, "speedup_vs_plain": ms_p / ms_b,
         "modmul_per_s": modmuls * steps / (ms_b * 1e-3), "bit_exact_vs_plain": exact,
     }
@@ -1078,7 +1078,7 @@ def run_single_config(args):
                                 cpu_sample=not args.no_cpu_baseline)
             metric = "BN254-Fr polynomial product coefficients/s (2^23 x 2^23 coefficients)"
         else:
-            r = run_lde_config(z, torch, stream, steps=args.steps, warmup=args.warmup, jobs=args.lde_jobs)
+            r = run_lde_config(z, torch, stream, steps=args.steps, warmup=args.warmup, count=args.lde_jobs)
             metric = f"batched coset LDE output elems/s ({args.lde_jobs} x 2^18 -> 2^20, BLS12-381-Fr)"
     line = {"metric": metric, "value": r["value"], "unit": r["unit"], "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "data": "synthetic: seeded inputs",
