@@ -99,7 +99,12 @@ static void* batch_shape_ptr(bool ext, bool full) {
 
 template <class F>
 static void* batch_kernel_ptr(int shape, bool ext, bool full) {
-  return shape == 0 ? batch_shape_ptr<F, 0>(ext, full) : batch_shape_ptr<F, 1>(ext, full);
+  switch (shape) {
+    case 0: return batch_shape_ptr<F, 0>(ext, full);
+    case 1: return batch_shape_ptr<F, 1>(ext, full);
+    case 2: return batch_shape_ptr<F, 2>(ext, full);
+    default: return batch_shape_ptr<F, 3>(ext, full);
+  }
 }
 
 cudaError_t configure_batch_kernels() {
@@ -150,8 +155,12 @@ static void launch_batch_shape(bool ext, bool full, const BatchPass* passes, con
 template <class F>
 static void launch_batch_typed(int shape, bool ext, bool full, const BatchPass* passes, const BatchItem* items,
                                uint32_t n_items, uint32_t* ctl, uint32_t spin_limit, int grid, cudaStream_t st) {
-  if (shape == 0) launch_batch_shape<F, 0>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st);
-  else launch_batch_shape<F, 1>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st);
+  switch (shape) {
+    case 0: launch_batch_shape<F, 0>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st); break;
+    case 1: launch_batch_shape<F, 1>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st); break;
+    case 2: launch_batch_shape<F, 2>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st); break;
+    default: launch_batch_shape<F, 3>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st); break;
+  }
 }
 
 cudaError_t launch_batch(int field, int shape, bool ext, bool full, const BatchPass* passes, const BatchItem* items,

@@ -39,6 +39,8 @@ template <class F>
 static cudaError_t set_pass_attrs() {
   cudaError_t e = set_shape_attrs<F, 0>();
   if (e == cudaSuccess) e = set_shape_attrs<F, 1>();
+  if (e == cudaSuccess) e = set_shape_attrs<F, 2>();
+  if (e == cudaSuccess) e = set_shape_attrs<F, 3>();
   return e;
 }
 
@@ -67,8 +69,12 @@ static void launch_pass_shape(bool ext, const PassParams& pp, dim3 grid, cudaStr
 
 template <class F>
 static void launch_pass_typed(int shape, bool ext, const PassParams& pp, dim3 grid, cudaStream_t st) {
-  if (shape == 0) launch_pass_shape<F, 0>(ext, pp, grid, st);
-  else launch_pass_shape<F, 1>(ext, pp, grid, st);
+  switch (shape) {
+    case 0: launch_pass_shape<F, 0>(ext, pp, grid, st); break;
+    case 1: launch_pass_shape<F, 1>(ext, pp, grid, st); break;
+    case 2: launch_pass_shape<F, 2>(ext, pp, grid, st); break;
+    default: launch_pass_shape<F, 3>(ext, pp, grid, st); break;
+  }
 }
 
 cudaError_t launch_ntt_pass(int field, int shape, const PassParams& pp, uint64_t num_tiles, cudaStream_t st) {
