@@ -43,46 +43,67 @@ __global__ void __launch_bounds__(THREADS, MINB)
                  uint32_t* ctl, uint32_t spin_limit) {
   extern __shared__ uint4 sm[];
   __shared__ PassParams s_pp;
-  __shared__ uint32_t s_item, s_ok;
+  __shared__ uint32_t s_item, s_ok, s_last;  // s_last: the pass whose parameters s_pp holds (warp 0)
   constexpr int kWords = sizeof(PassParams) / 4;
+  static_assert(kWords <= 32, "one warp copies a pass's parameters");
+  if (threadIdx.x == 0) s_last = kNoDep;
+  // Per item: warp 0 takes the next item (lane 0: one atomicAdd, and the
+  // bounded wait for the job's previous pass), copies the pass's parameters
+  // when they differ from the last item's, one barrier publishes both, the tile
+  // runs, and one barrier plus lane 0's release (fence, then the count) makes
+  // the tile's stores visible to the CTAs that wait for them -- the pattern of
+  // a cooperative grid barrier.  Two barriers and one fence per tile.
   for (;;) {
-    __syncthreads();  // the previous tile's shared-memory reads are done
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
       uint32_t it = n_items, ok = 1;
-      if (ld_relaxed(&ctl[1]) == 0) it = atomicAdd(&ctl[0], 1u);
-      if (it < n_items) {
-        const uint32_t dep = passes[items[it].pass].dep;
-        if (dep != kNoDep) {
-          const uint32_t need = passes[dep].tiles;
-          uint32_t spins = 0;
-          while (ld_acquire(&ctl[2 + dep]) < need) {
-            if (ld_relaxed(&ctl[1]) != 0) {
-              ok = 0;
-              break;
+      if (threadIdx.x == 0) {
+        if (ld_relaxed(&ctl[1]) == 0) it = atomicAdd(&ctl[0], 1u);
+        if (it < n_items) {
+          const uint32_t dep = passes[items[it].pass].dep;
+          if (dep != kNoDep) {
+            const uint32_t need = passes[dep].tiles;
+            uint32_t spins = 0;
+            while (ld_acquire(&ctl[2 + dep]) < need) {
+              if (ld_relaxed(&ctl[1]) != 0) {
+                ok = 0;
+                break;
+              }
+              if (++spins > spin_limit) {
+                atomicExch(&ctl[1], 1u);
+                ok = 0;
+                break;
+              }
+              __nanosleep(256);
             }
-            if (++spins > spin_limit) {
-              atomicExch(&ctl[1], 1u);
-              ok = 0;
-              break;
-            }
-            __nanosleep(256);
           }
         }
+        s_item = it;
+        s_ok = ok;
       }
-      s_item = it;
-      s_ok = ok;
+      it = __shfl_sync(0xffffffffu, it, 0);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (it < n_items && ok) {
+        const uint32_t pass = items[it].pass;
+        const uint32_t last = s_last;
+        __syncwarp();
+        if (pass != last) {
+          if (threadIdx.x < kWords)
+            reinterpret_cast<uint32_t*>(&s_pp)[threadIdx.x] =
+                reinterpret_cast<const uint32_t*>(&passes[pass].pp)[threadIdx.x];
+          if (threadIdx.x == 0) s_last = pass;
+        }
+      }
     }
     __syncthreads();
     const uint32_t it = s_item;
     if (it >= n_items || !s_ok) break;
     const BatchItem item = items[it];
-    const uint32_t* src = reinterpret_cast<const uint32_t*>(&passes[item.pass].pp);
-    for (int w = threadIdx.x; w < kWords; w += THREADS) reinterpret_cast<uint32_t*>(&s_pp)[w] = src[w];
-    __syncthreads();
     ntt_tile<F, LOG_TILE, THREADS, true, EXT, FULL>(s_pp, item.tile, sm);
-    __threadfence();  // this thread's stores are visible device-wide ...
-    __syncthreads();  // ... for every thread of the CTA, before the count
-    if (threadIdx.x == 0) atomicAdd(&ctl[2 + item.pass], 1u);
+    __syncthreads();  // every thread's stores are issued and its shared-memory reads done
+    if (threadIdx.x == 0) {
+      __threadfence();  // ... and, through the barrier, visible device-wide before the count
+      atomicAdd(&ctl[2 + item.pass], 1u);
+    }
   }
 }
 
