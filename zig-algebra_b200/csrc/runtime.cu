@@ -913,15 +913,21 @@ int zntt_probe_imad(double* per_second) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   ZCHECK(launch_imad_probe((uint32_t*)sink.p, 64, blocks, threads, c.stream), "imad probe");  // warm-up
-  cudaEventRecord(e0, c.stream);
-  ZCHECK(launch_imad_probe((uint32_t*)sink.p, iters, blocks, threads, c.stream), "imad probe");
-  cudaEventRecord(e1, c.stream);
-  ZCHECK(cudaEventSynchronize(e1), "imad probe");
-  float ms = 0;
-  cudaEventElapsedTime(&ms, e0, e1);
+  // The fastest of five timed launches: the peak is a capability, and a single
+  // 0.5 ms launch read up to 3% low on some boxes.
+  float best = 0;
+  for (int r = 0; r < 5; r++) {
+    cudaEventRecord(e0, c.stream);
+    ZCHECK(launch_imad_probe((uint32_t*)sink.p, iters, blocks, threads, c.stream), "imad probe");
+    cudaEventRecord(e1, c.stream);
+    ZCHECK(cudaEventSynchronize(e1), "imad probe");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r == 0 || ms < best) best = ms;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  *per_second = (double)blocks * threads * iters * 8.0 / (ms * 1e-3);
+  *per_second = (double)blocks * threads * iters * 8.0 / (best * 1e-3);
   return ZNTT_OK;
 }
 
