@@ -57,17 +57,14 @@ const SmallHost& small_host(int field) { return field == kGoldilocksField ? kGol
 constexpr int kSmallLogTile = 12;
 constexpr int kSmallThreads = 256;
 constexpr uint32_t kSmallKmax = 10;  // keeps 2^(12 - k) >= 4 columns (32-byte rows) per tile row
-// Transforms of 2^21 elements and more run on 2^11-element tiles in CTAs of
-// 128 threads: the same warps per SM in smaller CTAs, whose barriers wait on
-// fewer warps.  Goldilocks keeps radix-4 groups (2^24: 7.7% faster than 2^12
-// tiles in 256 threads, B200); BabyBear, whose products are cheap, uses
-// register groups of 16 elements, four stages per shared-memory round trip
-// (2^24: 0.350 against 0.375 ms).
+// Goldilocks transforms of 2^21 elements and more run on 2^11-element tiles in
+// CTAs of 128 threads (10 per SM): the same warps per SM in smaller CTAs, whose
+// barriers wait on fewer warps (2^24: 7.7% faster than 2^12 tiles in 256
+// threads, B200).  BabyBear gains nothing from it and keeps the larger tile.
 constexpr int kSmallLogTileB = 11;
 constexpr int kSmallThreadsB = 128;
 constexpr uint32_t kSmallKmaxB = 9;  // keeps 32-byte rows on 2^11-element tiles
-constexpr int kBabyBearMaxGroupB = 16;
-bool small_use_b(int, uint32_t log_n) { return log_n >= 21; }
+bool small_use_b(int field, uint32_t log_n) { return field == kGoldilocksField && log_n >= 21; }
 
 struct SmallPass {
   const uint64_t* src;
@@ -100,53 +97,12 @@ __device__ __forceinline__ void small_butterfly(uint64_t& u, uint64_t& v, bool m
   u = SF::add(u, t);
 }
 
-// Stages i .. i + log2(M) - 1 of a whole tile on groups of M elements held in
-// registers (radix-M): a group is the M positions t0 + s * 2^(i-1) of one tile
-// column; stage i + b pairs s and s + 2^b with the factor of butterfly index
-// j + (s mod 2^b) 2^(i-1).  One shared-memory round trip and one barrier per
-// log2(M) stages.
-template <class SF, int LOG_TILE, int THREADS, int M>
-__device__ __forceinline__ void small_group_round(const SmallPass& pp, uint32_t i, uint64_t* sm, uint32_t m0) {
-  constexpr int LOGM = M == 2 ? 1 : M == 4 ? 2 : M == 8 ? 3 : 4;
-  const uint32_t c = pp.c, C = 1u << c, h = 1u << (i - 1);
-#pragma unroll
-  for (uint32_t q = 0; q < (1u << LOG_TILE) / M / THREADS; q++) {
-    const uint32_t ga = threadIdx.x + q * THREADS;
-    const uint32_t col = ga & (C - 1), g = ga >> c;
-    const uint32_t j = g & (h - 1);
-    const uint32_t t0 = ((g >> (i - 1)) << (i - 1 + LOGM)) | j;
-    uint64_t x[M];
-#pragma unroll
-    for (int s = 0; s < M; s++) x[s] = sm[((t0 + s * h) << c) | col];
-#pragma unroll
-    for (int b = 0; b < LOGM; b++) {
-      const uint32_t half = 1u << (pp.S + i - 1 + b);
-      const uint64_t* stw = pp.tw + (half - 1);
-#pragma unroll
-      for (int s = 0; s < M; s++) {
-        if (s & (1 << b)) continue;
-        const uint32_t jj = j + (uint32_t)(s & ((1 << b) - 1)) * h;
-        const uint32_t jg = pp.first ? jj : (jj << pp.S) + m0 + col;
-        uint64_t w = 0;
-        const bool mul = small_twiddle<SF>(pp, stw, half, jg, w);
-        small_butterfly<SF>(x[s], x[s + (1 << b)], mul, w);
-      }
-    }
-#pragma unroll
-    for (int s = 0; s < M; s++) sm[((t0 + s * h) << c) | col] = x[s];
-  }
-  __syncthreads();
-}
-
 // One tile of one pass.  PAD: the first pass reads natural indices at or
 // beyond pp.src_len as zeros (a zero-padded input that is not stored).  FULL:
 // the tile is the whole 2^LOG_TILE (k + c == LOG_TILE), so no bound checks
 // (2^24 BabyBear about 10% faster without them on B200).
-// MAXM > 4 (whole tiles only): the stages run in register groups of up to
-// MAXM elements (small_group_round) instead of radix-4 groups.
-template <class SF, int LOG_TILE, int THREADS, bool PAD, bool FULL = false, int MAXM = 4>
+template <class SF, int LOG_TILE, int THREADS, bool PAD, bool FULL = false>
 __device__ __forceinline__ void small_pass_body(const SmallPass& pp, uint32_t blk, uint64_t* sm) {
-  static_assert(MAXM == 4 || FULL, "register groups wider than 4 need whole tiles");
   constexpr uint32_t TILE_MAX = 1u << LOG_TILE;
   const uint32_t k = pp.k, c = pp.c, C = 1u << c;
   const uint32_t tile = FULL ? TILE_MAX : 1u << (k + c);
@@ -179,83 +135,64 @@ __device__ __forceinline__ void small_pass_body(const SmallPass& pp, uint32_t bl
   }
   __syncthreads();
 
-  if constexpr (MAXM > 4) {
-    for (uint32_t i = 1; i <= k;) {
-      const uint32_t left = k - i + 1;
-      if (MAXM >= 16 && left >= 4) {
-        small_group_round<SF, LOG_TILE, THREADS, 16>(pp, i, sm, m0);
-        i += 4;
-      } else if (left >= 3) {
-        small_group_round<SF, LOG_TILE, THREADS, 8>(pp, i, sm, m0);
-        i += 3;
-      } else if (left == 2) {
-        small_group_round<SF, LOG_TILE, THREADS, 4>(pp, i, sm, m0);
-        i += 2;
-      } else {
-        small_group_round<SF, LOG_TILE, THREADS, 2>(pp, i, sm, m0);
-        i += 1;
+  uint32_t i = 1;
+  if (k & 1) {
+    const uint32_t half = 1u << pp.S;
+    const uint64_t* stw = pp.tw + (half - 1);
+#pragma unroll
+    for (uint32_t q = 0; q < TILE_MAX / 2 / THREADS; q++) {
+      const uint32_t b = tid + q * THREADS;
+      if (FULL || b < tile / 2) {
+        const uint32_t col = b & (C - 1), t0 = (b >> c) << 1;
+        const uint32_t jg = pp.first ? 0 : m0 + col;
+        const uint32_t e0 = (t0 << c) | col, e1 = e0 + C;
+        uint64_t u = sm[e0], v = sm[e1], w = 0;
+        const bool mul = small_twiddle<SF>(pp, stw, half, jg, w);
+        small_butterfly<SF>(u, v, mul, w);
+        sm[e0] = u;
+        sm[e1] = v;
       }
     }
-  } else {
-    uint32_t i = 1;
-    if (k & 1) {
-      const uint32_t half = 1u << pp.S;
-      const uint64_t* stw = pp.tw + (half - 1);
-  #pragma unroll
-      for (uint32_t q = 0; q < TILE_MAX / 2 / THREADS; q++) {
-        const uint32_t b = tid + q * THREADS;
-        if (FULL || b < tile / 2) {
-          const uint32_t col = b & (C - 1), t0 = (b >> c) << 1;
-          const uint32_t jg = pp.first ? 0 : m0 + col;
-          const uint32_t e0 = (t0 << c) | col, e1 = e0 + C;
-          uint64_t u = sm[e0], v = sm[e1], w = 0;
-          const bool mul = small_twiddle<SF>(pp, stw, half, jg, w);
-          small_butterfly<SF>(u, v, mul, w);
-          sm[e0] = u;
-          sm[e1] = v;
+    __syncthreads();
+    i = 2;
+  }
+  for (; i < k; i += 2) {
+    const uint32_t h = 1u << (i - 1);
+    const uint32_t half1 = 1u << (pp.S + i - 1), half2 = half1 << 1;
+    const uint64_t* stw1 = pp.tw + (half1 - 1);
+    const uint64_t* stw2 = pp.tw + (half2 - 1);
+#pragma unroll
+    for (uint32_t q = 0; q < TILE_MAX / 4 / THREADS; q++) {
+      const uint32_t ga = tid + q * THREADS;
+      if (FULL || ga < tile / 4) {
+        const uint32_t col = ga & (C - 1), g = ga >> c;
+        const uint32_t j = g & (h - 1);
+        const uint32_t t0 = ((g >> (i - 1)) << (i + 1)) | j;
+        const uint32_t e0 = (t0 << c) | col, eh = h << c;
+        uint32_t jg1, jg3;
+        if (pp.first) {
+          jg1 = j;
+          jg3 = j + h;
+        } else {
+          jg1 = (j << pp.S) + m0 + col;
+          jg3 = jg1 + (h << pp.S);
         }
+        uint64_t w1 = 0, w2 = 0, w3 = 0;
+        const bool m1 = small_twiddle<SF>(pp, stw1, half1, jg1, w1);
+        const bool m2 = small_twiddle<SF>(pp, stw2, half2, jg1, w2);
+        const bool m3 = small_twiddle<SF>(pp, stw2, half2, jg3, w3);
+        uint64_t x0 = sm[e0], x1 = sm[e0 + eh], x2 = sm[e0 + 2 * eh], x3 = sm[e0 + 3 * eh];
+        small_butterfly<SF>(x0, x1, m1, w1);
+        small_butterfly<SF>(x2, x3, m1, w1);
+        small_butterfly<SF>(x0, x2, m2, w2);
+        small_butterfly<SF>(x1, x3, m3, w3);
+        sm[e0] = x0;
+        sm[e0 + eh] = x1;
+        sm[e0 + 2 * eh] = x2;
+        sm[e0 + 3 * eh] = x3;
       }
-      __syncthreads();
-      i = 2;
     }
-    for (; i < k; i += 2) {
-      const uint32_t h = 1u << (i - 1);
-      const uint32_t half1 = 1u << (pp.S + i - 1), half2 = half1 << 1;
-      const uint64_t* stw1 = pp.tw + (half1 - 1);
-      const uint64_t* stw2 = pp.tw + (half2 - 1);
-  #pragma unroll
-      for (uint32_t q = 0; q < TILE_MAX / 4 / THREADS; q++) {
-        const uint32_t ga = tid + q * THREADS;
-        if (FULL || ga < tile / 4) {
-          const uint32_t col = ga & (C - 1), g = ga >> c;
-          const uint32_t j = g & (h - 1);
-          const uint32_t t0 = ((g >> (i - 1)) << (i + 1)) | j;
-          const uint32_t e0 = (t0 << c) | col, eh = h << c;
-          uint32_t jg1, jg3;
-          if (pp.first) {
-            jg1 = j;
-            jg3 = j + h;
-          } else {
-            jg1 = (j << pp.S) + m0 + col;
-            jg3 = jg1 + (h << pp.S);
-          }
-          uint64_t w1 = 0, w2 = 0, w3 = 0;
-          const bool m1 = small_twiddle<SF>(pp, stw1, half1, jg1, w1);
-          const bool m2 = small_twiddle<SF>(pp, stw2, half2, jg1, w2);
-          const bool m3 = small_twiddle<SF>(pp, stw2, half2, jg3, w3);
-          uint64_t x0 = sm[e0], x1 = sm[e0 + eh], x2 = sm[e0 + 2 * eh], x3 = sm[e0 + 3 * eh];
-          small_butterfly<SF>(x0, x1, m1, w1);
-          small_butterfly<SF>(x2, x3, m1, w1);
-          small_butterfly<SF>(x0, x2, m2, w2);
-          small_butterfly<SF>(x1, x3, m3, w3);
-          sm[e0] = x0;
-          sm[e0 + eh] = x1;
-          sm[e0 + 2 * eh] = x2;
-          sm[e0 + 3 * eh] = x3;
-        }
-      }
-      __syncthreads();
-    }
+    __syncthreads();
   }
 
 #pragma unroll
@@ -272,22 +209,22 @@ __device__ __forceinline__ void small_pass_body(const SmallPass& pp, uint32_t bl
   }
 }
 
-template <class SF, int LOG_TILE, int THREADS, bool FULL, int MAXM = 4>
+template <class SF, int LOG_TILE, int THREADS, bool FULL>
 __global__ void __launch_bounds__(THREADS) small_pass_kernel(SmallPass pp) {
   __shared__ uint64_t sm[1u << LOG_TILE];
-  small_pass_body<SF, LOG_TILE, THREADS, false, FULL, MAXM>(pp, blockIdx.x, sm);
+  small_pass_body<SF, LOG_TILE, THREADS, false, FULL>(pp, blockIdx.x, sm);
 }
 
 // The same pass over many columns of one size: column blockIdx.y reads
 // srcs[y] and writes dsts[y] (device pointer tables).
-template <class SF, int LOG_TILE, int THREADS, bool FULL, int MAXM = 4>
+template <class SF, int LOG_TILE, int THREADS, bool FULL>
 __global__ void __launch_bounds__(THREADS) small_pass_cols_kernel(SmallPass pp, const uint64_t* const* srcs,
                                                                   uint64_t* const* dsts) {
   __shared__ uint64_t sm[1u << LOG_TILE];
   SmallPass q = pp;
   q.src = srcs[blockIdx.y];
   q.dst = dsts[blockIdx.y];
-  small_pass_body<SF, LOG_TILE, THREADS, true, FULL, MAXM>(q, blockIdx.x, sm);
+  small_pass_body<SF, LOG_TILE, THREADS, true, FULL>(q, blockIdx.x, sm);
 }
 
 // Flat table entry e = 2^s - 1 + j holds root^(j * 2^(log_n - 1 - s)), in
@@ -392,14 +329,10 @@ static void launch_small_pass_t(const SmallPass& pp, uint64_t tiles, cudaStream_
 
 cudaError_t launch_small_pass(int field, const SmallPass& pp, uint64_t tiles, cudaStream_t st) {
   const bool full = pp.k + pp.c == (uint32_t)kSmallLogTile;
-  if (pp.k + pp.c == (uint32_t)kSmallLogTileB) {
+  if (field == kGoldilocksField && pp.k + pp.c == (uint32_t)kSmallLogTileB) {
     // a whole 2^11-element tile: the smaller CTA
-    if (field == kGoldilocksField)
-      small_pass_kernel<Goldilocks, kSmallLogTileB, kSmallThreadsB, true>
-          <<<(unsigned)tiles, kSmallThreadsB, 0, st>>>(pp);
-    else
-      small_pass_kernel<BabyBear, kSmallLogTileB, kSmallThreadsB, true, kBabyBearMaxGroupB>
-          <<<(unsigned)tiles, kSmallThreadsB, 0, st>>>(pp);
+    small_pass_kernel<Goldilocks, kSmallLogTileB, kSmallThreadsB, true>
+        <<<(unsigned)tiles, kSmallThreadsB, 0, st>>>(pp);
     return cudaGetLastError();
   }
   if (field == kGoldilocksField) {
@@ -416,13 +349,9 @@ cudaError_t launch_small_pass_cols(int field, const SmallPass& pp, uint64_t tile
                                    const uint64_t* const* srcs, uint64_t* const* dsts, cudaStream_t st) {
   const dim3 grid((unsigned)tiles, m);
   const bool full = pp.k + pp.c == (uint32_t)kSmallLogTile;
-  if (pp.k + pp.c == (uint32_t)kSmallLogTileB) {
-    if (field == kGoldilocksField)
-      small_pass_cols_kernel<Goldilocks, kSmallLogTileB, kSmallThreadsB, true>
-          <<<grid, kSmallThreadsB, 0, st>>>(pp, srcs, dsts);
-    else
-      small_pass_cols_kernel<BabyBear, kSmallLogTileB, kSmallThreadsB, true, kBabyBearMaxGroupB>
-          <<<grid, kSmallThreadsB, 0, st>>>(pp, srcs, dsts);
+  if (field == kGoldilocksField && pp.k + pp.c == (uint32_t)kSmallLogTileB) {
+    small_pass_cols_kernel<Goldilocks, kSmallLogTileB, kSmallThreadsB, true>
+        <<<grid, kSmallThreadsB, 0, st>>>(pp, srcs, dsts);
     return cudaGetLastError();
   }
   if (field == kGoldilocksField) {
