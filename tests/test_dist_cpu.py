@@ -63,3 +63,22 @@ def test_reference_arm_under_torchrun_rank0_only():
     lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
     assert lines[0]["impl"] == "reference" and lines[0]["value"] > 0
+
+
+def test_summary_digests_every_configuration():
+    """bench.py ends its line with a short digest of every configuration; the digest reads the
+    keys the configurations write (a renamed key would break the default run on the GPU)."""
+    import bench
+    cfg = {"ms_per_batch": 3.0, "plain_ms_per_batch": 15.0, "speedup_vs_plain": 5.0, "bit_exact_vs_plain": True}
+    served = {"p50_ms": 0.12, "p99_ms": 3.0, "throughput_req_s": 2000.0, "mismatches": 0, "failures": 0}
+    line = {"ms_per_step": 3.54, "roofline": {"frac": 0.845},
+            "e2e": {"value": 1.4e9, "pcie": {"e2e_frac_of_bound": 0.94}},
+            "sizes": {"bn254_fr 2^24 forward": {"ms": 3.54, "frac": 0.845}},
+            "batched": cfg, "coset_lde": cfg,
+            "serve": {"continuous_batching": served, "serial_plain": dict(served, p50_ms=0.13)},
+            "poly_mul": {"ms": 11.4}, "small_fields": {"fields": {"goldilocks": {"ms": 0.52}}}}
+    s = bench.summarize(line)
+    assert s["headline"]["frac"] == 0.845 and s["batched"]["speedup_vs_plain"] == 5.0
+    assert s["serve"]["serial_p50_ms"] == 0.13 and s["serve"]["mismatches"] == 0
+    assert s["sizes_ms_frac"]["bn254_fr 2^24 forward"] == [3.54, 0.845]
+    assert len(json.dumps(s)) < 1400  # it must fit the end of the line that readers keep
