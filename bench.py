@@ -15,7 +15,8 @@ beside it one synchronous zntt_ntt_with_twiddles call.  Under torchrun every
 rank transforms its own vector (independent objects: weak scaling, no
 collective on the data path); the time is the max over ranks.  `e2e.pcie`
 measures the host link's duplex bound beside it.  The default run adds, on
-rank 0, one key per configuration beside the headline: sizes (BN254-Fr 2^20,
+a single-GPU run, one key per configuration beside the headline (a multi-GPU run prints the
+headline and e2e only): sizes (BN254-Fr 2^20,
 2^22, 2^24 and BLS12-381-Fr 2^24, forward and inverse, each with its fraction of
 the multiply-pipe roofline), batched, coset_lde, poly_mul, small_fields --
 transforms, an extension, a 64-column trace extension and row commitment --,
@@ -371,9 +372,10 @@ def run_zntt(args, rank, world, local):
     traffic = read_traffic(log_n)
     tw.close()
     extra = {}
-    # The configurations beside the headline run once, on rank 0 (the other ranks wait at the
-    # closing barrier, well inside its timeout): they describe the library, not the scaling.
-    if not args.headline_only and rank == 0:
+    # The configurations beside the headline run once, in a single-GPU run: they describe the
+    # library, not the scaling, and under torchrun the other ranks would wait for them at the
+    # closing barrier for longer than the process group's timeout.
+    if not args.headline_only and world == 1:
         with torch.cuda.stream(stream):
             extra["sizes"] = run_size_sweep(z, torch, stream, steps=10, warmup=3, peak_modmul=peak_modmul)
             extra["batched"] = run_batched_config(z, torch, stream, steps=20, warmup=3)
