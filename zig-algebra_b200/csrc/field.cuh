@@ -40,6 +40,9 @@ namespace zntt {
 //           product; Q0..Q7 are the limbs of 2p.
 //   kSplit  product form: split accumulators (fe_mul_split) or merged rows
 //           (fe_mul_merged).
+//   kScaleCompiled  the pass kernel keeps its output-scaling code in every
+//           pass, also where no pass scales: the register allocation it gets
+//           times faster for this field (B200).
 // The special low limbs of both primes (BN254-Fr: p0 = 2^32 - 2^28 + 1;
 // BLS12-381-Fr: p0 = 1, p1 = 2^32 - 1) allow a reduction from shifts and adds
 // with fewer products.  It times faster alone but slower in the pass kernel,
@@ -48,6 +51,7 @@ struct Bn254Fr {
   static constexpr int kId = 0;
   static constexpr bool kLazy = true;
   static constexpr bool kSplit = false;
+  static constexpr bool kScaleCompiled = false;
   static constexpr uint32_t P0 = 0xf0000001u, P1 = 0x43e1f593u, P2 = 0x79b97091u, P3 = 0x2833e848u,
                             P4 = 0x8181585du, P5 = 0xb85045b6u, P6 = 0xe131a029u, P7 = 0x30644e72u;
   static constexpr uint32_t Q0 = P0 << 1, Q1 = (P1 << 1) | (P0 >> 31), Q2 = (P2 << 1) | (P1 >> 31),
@@ -67,6 +71,7 @@ struct Bls12381Fr {
   static constexpr int kId = 1;
   static constexpr bool kLazy = false;  // 4p > 2^256
   static constexpr bool kSplit = true;
+  static constexpr bool kScaleCompiled = true;
   static constexpr uint32_t P0 = 0x00000001u, P1 = 0xffffffffu, P2 = 0xfffe5bfeu, P3 = 0x53bda402u,
                             P4 = 0x09a1d805u, P5 = 0x3339d808u, P6 = 0x299d7d48u, P7 = 0x73eda753u;
   static constexpr uint32_t N0 = 0xffffffffu;

@@ -13,22 +13,26 @@
 
 namespace zntt {
 
-template <class F, int LOG_TILE, int THREADS, int MINB, bool EXT, bool FULL>
+// SCALE: the pass scales its outputs (the inverse's last pass, or an
+// extension pass); the extension variants always include it.
+template <class F, int LOG_TILE, int THREADS, int MINB, bool EXT, bool FULL, bool SCALE>
 __global__ void __launch_bounds__(THREADS, MINB) ntt_pass_kernel(PassParams pp) {
   extern __shared__ uint4 sm[];
-  ntt_tile<F, LOG_TILE, THREADS, false, EXT, FULL>(pp, blockIdx.x, sm);
+  ntt_tile<F, LOG_TILE, THREADS, false, EXT, FULL, SCALE>(pp, blockIdx.x, sm);
 }
 
-template <class F, int SH, bool EXT, bool FULL>
+template <class F, int SH, bool EXT, bool FULL, bool SCALE>
 static void* pass_ptr() {
-  return (void*)ntt_pass_kernel<F, kShapes[SH].log_tile, kShapes[SH].threads, kShapes[SH].min_blocks, EXT, FULL>;
+  return (void*)ntt_pass_kernel<F, kShapes[SH].log_tile, kShapes[SH].threads, kShapes[SH].min_blocks, EXT, FULL,
+                                SCALE>;
 }
 
 template <class F, int SH>
 static cudaError_t set_shape_attrs() {
-  void* fns[4] = {pass_ptr<F, SH, false, false>(), pass_ptr<F, SH, true, false>(), pass_ptr<F, SH, false, true>(),
-                  pass_ptr<F, SH, true, true>()};
-  for (int i = 0; i < 4; i++) {
+  void* fns[6] = {pass_ptr<F, SH, false, false, false>(), pass_ptr<F, SH, false, false, true>(),
+                  pass_ptr<F, SH, false, true, false>(),  pass_ptr<F, SH, false, true, true>(),
+                  pass_ptr<F, SH, true, false, true>(),   pass_ptr<F, SH, true, true, true>()};
+  for (int i = 0; i < 6; i++) {
     cudaError_t e = cudaFuncSetAttribute(fns[i], cudaFuncAttributeMaxDynamicSharedMemorySize, shape_smem_bytes(SH));
     if (e != cudaSuccess) return e;
   }
@@ -54,10 +58,14 @@ cudaError_t configure_kernels() {
 template <class F, int SH, bool FULL>
 static void launch_pass_full(bool ext, const PassParams& pp, dim3 grid, cudaStream_t st) {
   constexpr PassShape S = kShapes[SH];
+  constexpr int T = S.threads;
+  const int smem = shape_smem_bytes(SH);
   if (ext)
-    ntt_pass_kernel<F, S.log_tile, S.threads, S.min_blocks, true, FULL><<<grid, S.threads, shape_smem_bytes(SH), st>>>(pp);
+    ntt_pass_kernel<F, S.log_tile, T, S.min_blocks, true, FULL, true><<<grid, T, smem, st>>>(pp);
+  else if (pp.scale || F::kScaleCompiled)
+    ntt_pass_kernel<F, S.log_tile, T, S.min_blocks, false, FULL, true><<<grid, T, smem, st>>>(pp);
   else
-    ntt_pass_kernel<F, S.log_tile, S.threads, S.min_blocks, false, FULL><<<grid, S.threads, shape_smem_bytes(SH), st>>>(pp);
+    ntt_pass_kernel<F, S.log_tile, T, S.min_blocks, false, FULL, false><<<grid, T, smem, st>>>(pp);
 }
 
 template <class F, int SH>
