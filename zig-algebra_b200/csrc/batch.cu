@@ -124,7 +124,8 @@ static void* batch_kernel_ptr(int shape, bool ext, bool full) {
     case 0: return batch_shape_ptr<F, 0>(ext, full);
     case 1: return batch_shape_ptr<F, 1>(ext, full);
     case 2: return batch_shape_ptr<F, 2>(ext, full);
-    default: return batch_shape_ptr<F, 3>(ext, full);
+    case 3: return batch_shape_ptr<F, 3>(ext, full);
+    default: return batch_shape_ptr<F, 4>(ext, full);
   }
 }
 
@@ -180,7 +181,8 @@ static void launch_batch_typed(int shape, bool ext, bool full, const BatchPass* 
     case 0: launch_batch_shape<F, 0>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st); break;
     case 1: launch_batch_shape<F, 1>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st); break;
     case 2: launch_batch_shape<F, 2>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st); break;
-    default: launch_batch_shape<F, 3>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st); break;
+    case 3: launch_batch_shape<F, 3>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st); break;
+    default: launch_batch_shape<F, 4>(ext, full, passes, items, n_items, ctl, spin_limit, grid, st); break;
   }
 }
 

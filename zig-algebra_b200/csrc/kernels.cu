@@ -45,6 +45,7 @@ static cudaError_t set_pass_attrs() {
   if (e == cudaSuccess) e = set_shape_attrs<F, 1>();
   if (e == cudaSuccess) e = set_shape_attrs<F, 2>();
   if (e == cudaSuccess) e = set_shape_attrs<F, 3>();
+  if (e == cudaSuccess) e = set_shape_attrs<F, 4>();
   return e;
 }
 
@@ -81,7 +82,8 @@ static void launch_pass_typed(int shape, bool ext, const PassParams& pp, dim3 gr
     case 0: launch_pass_shape<F, 0>(ext, pp, grid, st); break;
     case 1: launch_pass_shape<F, 1>(ext, pp, grid, st); break;
     case 2: launch_pass_shape<F, 2>(ext, pp, grid, st); break;
-    default: launch_pass_shape<F, 3>(ext, pp, grid, st); break;
+    case 3: launch_pass_shape<F, 3>(ext, pp, grid, st); break;
+    default: launch_pass_shape<F, 4>(ext, pp, grid, st); break;
   }
 }
 
