@@ -192,7 +192,8 @@ typedef struct zntt_job {
 } zntt_job;
 typedef struct zntt_batch zntt_batch;
 
-/* Plans the jobs (shape: a pass shape index, or -1 for the tuned one) and
+/* Plans the jobs (shape: a pass shape index, or -1 for the library's batch
+ * shape, 2^9-element tiles at 7 CTAs per SM) and
  * uploads the work queue; buffers stay owned by the caller and must outlive
  * the batch. */
 int zntt_batch_create(int field, const zntt_job* jobs, size_t n_jobs, int shape, zntt_batch** out);

@@ -202,7 +202,6 @@ int zntt_batch_create(int field, const zntt_job* jobs, size_t n_jobs, int shape,
   if (c.device < 0) return set_error(ZNTT_ERR_NOT_INITIALIZED, "zntt_init has not been called");
   std::lock_guard<std::recursive_mutex> lock(c.mu);
   // Validate every job before allocating anything.
-  uint32_t biggest = 0;
   for (size_t j = 0; j < n_jobs; j++) {
     const zntt_job& job = jobs[j];
     if (!job.tw || !job.d_src || !job.d_dst) return set_error(ZNTT_ERR_INVALID_ARGUMENT, "job with a null pointer");
@@ -226,11 +225,10 @@ int zntt_batch_create(int field, const zntt_job* jobs, size_t n_jobs, int shape,
     } else {
       return set_error(ZNTT_ERR_INVALID_ARGUMENT, "unknown job kind");
     }
-    biggest = std::max(biggest, tw_of(job.tw)->log_n);
   }
   zntt_batch* b = new zntt_batch();
   b->field = field;
-  b->shape = shape >= 0 ? shape : tuned_plan(field, biggest).shape;
+  b->shape = shape >= 0 ? shape : kBatchShape;
   cudaStream_t st = c.stream;
 
   std::vector<JobPlan> plans(n_jobs);

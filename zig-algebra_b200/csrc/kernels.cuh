@@ -55,6 +55,12 @@ struct PassShape {
 // warps per SM: 2^22 and 2^24 BN254-Fr about 0.6% faster, BLS12-381-Fr slower.
 constexpr int kNumShapes = 5;
 constexpr PassShape kShapes[kNumShapes] = {{11, 256, 3}, {10, 256, 3}, {9, 128, 6}, {8, 64, 12}, {9, 128, 7}};
+// The shape of persistent launches (batches and the server's slices): the
+// 7-CTA 2^9 tile ran the mixed 520-transform batch 3.03 -> 2.94 ms and 64
+// coset extensions 2^18 -> 2^20 16.95 -> 16.74 ms (BLS12-381-Fr) and 15.81 ->
+// 15.45 ms (BN254-Fr) against the 6-CTA tile, and the 2^10 and 2^8 tiles
+// slower still (B200).
+constexpr int kBatchShape = 4;
 constexpr int kLogTile = 11;  // the largest tile of any shape
 constexpr int kDefaultShape = 0;
 

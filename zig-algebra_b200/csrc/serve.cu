@@ -113,7 +113,7 @@ static uint64_t plan_tiles(const Plan& p, uint32_t log_n) {
 }
 
 static void req_work(zntt_server* s, const zntt_request& r, uint64_t* items, uint32_t* passes) {
-  const int f = s->cfg.field, sh = kDefaultShape;
+  const int f = s->cfg.field, sh = kBatchShape;
   const Plan po = batch_plan(f, r.log_n, sh);
   *items = plan_tiles(po, r.log_n);
   *passes = po.np;
@@ -277,7 +277,7 @@ static bool launch_into(zntt_server* s, Slot& sl) {
 
   std::lock_guard<std::recursive_mutex> lock(ctx().mu);
   std::vector<JobPlan> plans(sl.reqs.size());
-  const int shape = kDefaultShape;
+  const int shape = kBatchShape;
   // One request alone runs as plain per-pass launches: the persistent launch
   // pays off only when several requests share it (its queue upload and launch
   // cost a lone small request about 60 us of latency).
@@ -363,8 +363,8 @@ static bool launch_into(zntt_server* s, Slot& sl) {
     if (ce == cudaSuccess) ce = cudaMemsetAsync(sl.d_ctl, 0, (2 + np) * 4, st);
     if (ce == cudaSuccess) {
       const int grid = std::max(1, std::min<int>(ext ? s->grid_ext : s->grid_plain, (int)ni));
-      const bool full = batch_all_full(kDefaultShape, sl.h_passes, np);
-      ce = launch_batch(field, kDefaultShape, ext, full, sl.d_passes, sl.d_items, ni, sl.d_ctl, ZNTT_BATCH_SPIN_LIMIT,
+      const bool full = batch_all_full(kBatchShape, sl.h_passes, np);
+      ce = launch_batch(field, kBatchShape, ext, full, sl.d_passes, sl.d_items, ni, sl.d_ctl, ZNTT_BATCH_SPIN_LIMIT,
                         grid, st);
     }
     if (ce == cudaSuccess) ce = cudaMemcpyAsync(sl.h_flag, sl.d_ctl + 1, 4, cudaMemcpyDeviceToHost, st);
@@ -462,8 +462,8 @@ int zntt_server_create(const zntt_server_config* cfg, zntt_server** out) {
   std::memset(&s->stats, 0, sizeof(s->stats));
   s->cap_items = s->cfg.max_items;
   s->cap_passes = (size_t)s->cfg.max_batch_jobs * 8;
-  s->grid_plain = batch_grid(cfg->field, kDefaultShape, false);
-  s->grid_ext = batch_grid(cfg->field, kDefaultShape, true);
+  s->grid_plain = batch_grid(cfg->field, kBatchShape, false);
+  s->grid_ext = batch_grid(cfg->field, kBatchShape, true);
   s->slots.resize(s->cfg.slots);
   cudaError_t ce = cudaSuccess;
   for (Slot& sl : s->slots) {
