@@ -35,13 +35,13 @@ __device__ __forceinline__ void sm_store(uint4* sm, uint32_t e, const fe& a) {
 // Twiddle of global stage s (1-based) for butterfly index jg, with the
 // forward (tw[s-1][jg]) or inttWithTwiddles (1 or -tw[s-1][2^(s-1) - jg])
 // mapping.  `stw` points at tw[s-1]; returns false when the factor is one and
-// the multiply can be skipped.  The inverse's factor is p - tw (fe_p_minus):
+// the multiply can be skipped (unit0: entry 0 is one, always so for the inverse).  The inverse's factor is p - tw (fe_p_minus):
 // the product equals the one by -tw mod p, also for a zero entry.
 template <class F>
-__device__ __forceinline__ bool twiddle(const PassParams& pp, const uint4* stw, uint64_t half_g, uint64_t jg,
+__device__ __forceinline__ bool twiddle(bool inverse, bool unit0, const uint4* stw, uint64_t half_g, uint64_t jg,
                                         fe& w) {
-  if (jg == 0 && (pp.inverse | pp.tw0_one)) return false;
-  if (!pp.inverse) {
+  if (jg == 0 && unit0) return false;
+  if (!inverse) {
     w = fe_load_nc(stw + (jg << 1));
   } else {
     w = fe_p_minus<F>(fe_load_nc(stw + ((half_g - jg) << 1)));
@@ -93,16 +93,21 @@ __device__ __forceinline__ uint4 load_data(const uint4* p) {
 template <class F, int LOG_TILE, int THREADS, bool COHERENT, bool EXT, bool FULL = false, bool SCALE = true>
 __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uint4* sm) {
   constexpr uint32_t TILE_MAX = 1u << LOG_TILE;
-  const uint32_t k = pp.k, c = pp.c, C = 1u << c;
+  // The fields the stage loop reads, read once (for parameters held in
+  // memory rather than in the kernel's parameter space, each later read would
+  // be a load re-issued after every barrier).
+  const uint32_t k = pp.k, c = pp.c, C = 1u << c, S = pp.S;
+  const bool first = pp.first, inverse = pp.inverse, unit0 = pp.inverse | pp.tw0_one;
+  const uint4* const tw = pp.tw;
   const uint32_t tile = FULL ? TILE_MAX : 1u << (k + c);
   const uint32_t tid = threadIdx.x;
 
   uint64_t hi_base = 0, m0 = 0, col0 = 0;
-  if (pp.first) {
+  if (first) {
     col0 = blk << c;
   } else {
-    const uint32_t mlog = pp.S - c;
-    hi_base = (blk >> mlog) << (pp.S + k);
+    const uint32_t mlog = S - c;
+    hi_base = (blk >> mlog) << (S + k);
     m0 = (blk & ((1ull << mlog) - 1)) << c;
   }
   const uint32_t xcols_log = pp.log_n - k;
@@ -117,13 +122,13 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
       uint64_t g;
       uint32_t t;
       uint4 val;
-      if (pp.first) {
+      if (first) {
         g = ((uint64_t)row << xcols_log) + col0 + col;
         t = rev_bits(row, k);
         if (EXT && g >= src_len) val = make_uint4(0, 0, 0, 0);
         else val = load_data<COHERENT>(pp.src + ((g << 1) | h));
       } else {
-        g = hi_base + ((uint64_t)row << pp.S) + m0 + col;
+        g = hi_base + ((uint64_t)row << S) + m0 + col;
         t = row;
         val = load_data<COHERENT>(pp.src + ((g << 1) | h));
       }
@@ -136,10 +141,10 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
   uint32_t i = 1;
   for (; i < k; i += 2) {
     const uint32_t h = 1u << (i - 1);
-    const uint64_t half1 = 1ull << (pp.S + i - 1);  // stage S+i
+    const uint64_t half1 = 1ull << (S + i - 1);  // stage S+i
     const uint64_t half2 = half1 << 1;              // stage S+i+1
-    const uint4* stw1 = pp.tw + ((half1 - 1) << 1);
-    const uint4* stw2 = pp.tw + ((half2 - 1) << 1);
+    const uint4* stw1 = tw + ((half1 - 1) << 1);
+    const uint4* stw2 = tw + ((half2 - 1) << 1);
 #pragma unroll
     for (uint32_t q = 0; q < TILE_MAX / 4 / THREADS; q++) {
       const uint32_t ga = tid + q * THREADS;
@@ -149,17 +154,17 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
         const uint32_t t0 = ((g >> (i - 1)) << (i + 1)) | j;
         const uint32_t e0 = (t0 << c) | col, eh = h << c;
         uint64_t jg1, jg3;
-        if (pp.first) {
+        if (first) {
           jg1 = j;
           jg3 = j + h;
         } else {
-          jg1 = ((uint64_t)j << pp.S) + m0 + col;
-          jg3 = jg1 + ((uint64_t)h << pp.S);
+          jg1 = ((uint64_t)j << S) + m0 + col;
+          jg3 = jg1 + ((uint64_t)h << S);
         }
         fe w1, w2, w3;
-        const bool m1 = twiddle<F>(pp, stw1, half1, jg1, w1);
-        const bool m2 = twiddle<F>(pp, stw2, half2, jg1, w2);
-        const bool m3 = twiddle<F>(pp, stw2, half2, jg3, w3);
+        const bool m1 = twiddle<F>(inverse, unit0, stw1, half1, jg1, w1);
+        const bool m2 = twiddle<F>(inverse, unit0, stw2, half2, jg1, w2);
+        const bool m3 = twiddle<F>(inverse, unit0, stw2, half2, jg3, w3);
         fe x0 = sm_load<TILE_MAX>(sm, e0), x1 = sm_load<TILE_MAX>(sm, e0 + eh),
            x2 = sm_load<TILE_MAX>(sm, e0 + 2 * eh), x3 = sm_load<TILE_MAX>(sm, e0 + 3 * eh);
         butterfly<F>(x0, x1, m1, w1);
@@ -186,8 +191,8 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
   // pass skips their products in whole warps (2^20 first pass 8% faster, B200).
   if (k & 1) {
     const uint32_t h = 1u << (k - 1);
-    const uint64_t half_g = 1ull << (pp.S + k - 1);  // stage S+k
-    const uint4* stw = pp.tw + ((half_g - 1) << 1);
+    const uint64_t half_g = 1ull << (S + k - 1);  // stage S+k
+    const uint4* stw = tw + ((half_g - 1) << 1);
 #pragma unroll
     for (uint32_t q = 0; q < TILE_MAX / 2 / THREADS; q++) {
       const uint32_t b = tid + q * THREADS;
@@ -195,10 +200,10 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
         const uint32_t col = b & (C - 1), g = b >> c;
         const uint32_t j = g & (h - 1);
         const uint32_t t0 = ((g >> (k - 1)) << k) | j;
-        const uint64_t jg = pp.first ? (uint64_t)j : ((uint64_t)j << pp.S) + m0 + col;
+        const uint64_t jg = first ? (uint64_t)j : ((uint64_t)j << S) + m0 + col;
         const uint32_t e0 = (t0 << c) | col, e1 = e0 + (h << c);
         fe u = sm_load<TILE_MAX>(sm, e0), v = sm_load<TILE_MAX>(sm, e1), w;
-        const bool mul = twiddle<F>(pp, stw, half_g, jg, w);
+        const bool mul = twiddle<F>(inverse, unit0, stw, half_g, jg, w);
         butterfly<F>(u, v, mul, w);
         canonical<F>(u, true);
         canonical<F>(v, true);
@@ -220,8 +225,8 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
       if (FULL || e < tile) {
         const uint32_t col = e & (C - 1), row = e >> c;
         if (EXT && pp.scale_tab) {
-          const uint64_t g = pp.first ? ((uint64_t)rev_bits((uint32_t)(col0 + col), xcols_log) << k) + row
-                                      : hi_base + ((uint64_t)row << pp.S) + m0 + col;
+          const uint64_t g = first ? ((uint64_t)rev_bits((uint32_t)(col0 + col), xcols_log) << k) + row
+                                      : hi_base + ((uint64_t)row << S) + m0 + col;
           sc = fe_load_nc(pp.scale_tab + (g << 1));
         }
         sm_store<TILE_MAX>(sm, e, fe_mul<F>(sm_load<TILE_MAX>(sm, e), sc));
@@ -236,10 +241,10 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
     if (FULL || idx < 2 * tile) {
       const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
       uint64_t g;
-      if (pp.first) {
+      if (first) {
         g = ((uint64_t)rev_bits((uint32_t)(col0 + col), xcols_log) << k) + row;
       } else {
-        g = hi_base + ((uint64_t)row << pp.S) + m0 + col;
+        g = hi_base + ((uint64_t)row << S) + m0 + col;
       }
       if (!EXT || g < pp.dst_len) pp.dst[(g << 1) | h] = sm[h * TILE_MAX + ((row << c) | col)];
     }
