@@ -38,7 +38,7 @@ __device__ __forceinline__ void sm_store(uint4* sm, uint32_t e, const fe& a) {
 // the multiply can be skipped (unit0: entry 0 is one, always so for the inverse).  The inverse's factor is p - tw (fe_p_minus):
 // the product equals the one by -tw mod p, also for a zero entry.
 template <class F>
-__device__ __forceinline__ bool twiddle(bool inverse, bool unit0, const uint4* stw, uint64_t half_g, uint64_t jg,
+__device__ __forceinline__ bool twiddle(bool inverse, bool unit0, const uint4* stw, uint32_t half_g, uint32_t jg,
                                         fe& w) {
   if (jg == 0 && unit0) return false;
   if (!inverse) {
@@ -102,13 +102,16 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
   const uint32_t tile = FULL ? TILE_MAX : 1u << (k + c);
   const uint32_t tid = threadIdx.x;
 
-  uint64_t hi_base = 0, m0 = 0, col0 = 0;
+  // Indices fit 32 bits: transforms and tables hold at most 2^31 elements, so
+  // an element's 16-byte-half offset is below 2^32.
+  const uint32_t b = (uint32_t)blk;
+  uint32_t hi_base = 0, m0 = 0, col0 = 0;
   if (first) {
-    col0 = blk << c;
+    col0 = b << c;
   } else {
     const uint32_t mlog = S - c;
-    hi_base = (blk >> mlog) << (S + k);
-    m0 = (blk & ((1ull << mlog) - 1)) << c;
+    hi_base = (b >> mlog) << (S + k);
+    m0 = (b & ((1u << mlog) - 1)) << c;
   }
   const uint32_t xcols_log = pp.log_n - k;
   const uint64_t src_len = pp.src_len;
@@ -119,16 +122,15 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
     const uint32_t idx = tid + q * THREADS;
     if (FULL || idx < 2 * tile) {
       const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
-      uint64_t g;
-      uint32_t t;
+      uint32_t g, t;
       uint4 val;
       if (first) {
-        g = ((uint64_t)row << xcols_log) + col0 + col;
+        g = (row << xcols_log) + col0 + col;
         t = rev_bits(row, k);
         if (EXT && g >= src_len) val = make_uint4(0, 0, 0, 0);
         else val = load_data<COHERENT>(pp.src + ((g << 1) | h));
       } else {
-        g = hi_base + ((uint64_t)row << S) + m0 + col;
+        g = hi_base + (row << S) + m0 + col;
         t = row;
         val = load_data<COHERENT>(pp.src + ((g << 1) | h));
       }
@@ -141,8 +143,8 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
   uint32_t i = 1;
   for (; i < k; i += 2) {
     const uint32_t h = 1u << (i - 1);
-    const uint64_t half1 = 1ull << (S + i - 1);  // stage S+i
-    const uint64_t half2 = half1 << 1;              // stage S+i+1
+    const uint32_t half1 = 1u << (S + i - 1);  // stage S+i
+    const uint32_t half2 = half1 << 1;         // stage S+i+1
     const uint4* stw1 = tw + ((half1 - 1) << 1);
     const uint4* stw2 = tw + ((half2 - 1) << 1);
 #pragma unroll
@@ -153,13 +155,13 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
         const uint32_t j = g & (h - 1);
         const uint32_t t0 = ((g >> (i - 1)) << (i + 1)) | j;
         const uint32_t e0 = (t0 << c) | col, eh = h << c;
-        uint64_t jg1, jg3;
+        uint32_t jg1, jg3;
         if (first) {
           jg1 = j;
           jg3 = j + h;
         } else {
-          jg1 = ((uint64_t)j << S) + m0 + col;
-          jg3 = jg1 + ((uint64_t)h << S);
+          jg1 = (j << S) + m0 + col;
+          jg3 = jg1 + (h << S);
         }
         fe w1, w2, w3;
         const bool m1 = twiddle<F>(inverse, unit0, stw1, half1, jg1, w1);
@@ -191,7 +193,7 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
   // pass skips their products in whole warps (2^20 first pass 8% faster, B200).
   if (k & 1) {
     const uint32_t h = 1u << (k - 1);
-    const uint64_t half_g = 1ull << (S + k - 1);  // stage S+k
+    const uint32_t half_g = 1u << (S + k - 1);  // stage S+k
     const uint4* stw = tw + ((half_g - 1) << 1);
 #pragma unroll
     for (uint32_t q = 0; q < TILE_MAX / 2 / THREADS; q++) {
@@ -200,7 +202,7 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
         const uint32_t col = b & (C - 1), g = b >> c;
         const uint32_t j = g & (h - 1);
         const uint32_t t0 = ((g >> (k - 1)) << k) | j;
-        const uint64_t jg = first ? (uint64_t)j : ((uint64_t)j << S) + m0 + col;
+        const uint32_t jg = first ? j : (j << S) + m0 + col;
         const uint32_t e0 = (t0 << c) | col, e1 = e0 + (h << c);
         fe u = sm_load<TILE_MAX>(sm, e0), v = sm_load<TILE_MAX>(sm, e1), w;
         const bool mul = twiddle<F>(inverse, unit0, stw, half_g, jg, w);
@@ -225,8 +227,7 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
       if (FULL || e < tile) {
         const uint32_t col = e & (C - 1), row = e >> c;
         if (EXT && pp.scale_tab) {
-          const uint64_t g = first ? ((uint64_t)rev_bits((uint32_t)(col0 + col), xcols_log) << k) + row
-                                      : hi_base + ((uint64_t)row << S) + m0 + col;
+          const uint32_t g = first ? (rev_bits(col0 + col, xcols_log) << k) + row : hi_base + (row << S) + m0 + col;
           sc = fe_load_nc(pp.scale_tab + (g << 1));
         }
         sm_store<TILE_MAX>(sm, e, fe_mul<F>(sm_load<TILE_MAX>(sm, e), sc));
@@ -240,11 +241,11 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
     const uint32_t idx = tid + q * THREADS;
     if (FULL || idx < 2 * tile) {
       const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
-      uint64_t g;
+      uint32_t g;
       if (first) {
-        g = ((uint64_t)rev_bits((uint32_t)(col0 + col), xcols_log) << k) + row;
+        g = (rev_bits(col0 + col, xcols_log) << k) + row;
       } else {
-        g = hi_base + ((uint64_t)row << S) + m0 + col;
+        g = hi_base + (row << S) + m0 + col;
       }
       if (!EXT || g < pp.dst_len) pp.dst[(g << 1) | h] = sm[h * TILE_MAX + ((row << c) | col)];
     }
