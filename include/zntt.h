@@ -418,7 +418,8 @@ uint64_t zntt_now_ns(void);
 
 /* ---- autotuner ------------------------------------------------------------------
  * Times every pass shape and stage count per pass for each log n in
- * [log_n_min, log_n_max] on this GPU and keeps the fastest; plans use the
+ * [log_n_min, log_n_max] on this GPU, a forward and an inverse transform
+ * each (one plan serves both directions), and keeps the fastest; plans use the
  * table from then on.  The table persists as JSON lines keyed by GPU name;
  * zntt_init loads the file named by ZNTT_TUNE_FILE when it exists. */
 int zntt_autotune(int field, uint32_t log_n_min, uint32_t log_n_max);

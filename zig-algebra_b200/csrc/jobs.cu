@@ -530,6 +530,8 @@ int zntt_autotune(int field, uint32_t log_n_min, uint32_t log_n_max) {
     if (!rc) rc = pool_get((size_t)32 << L, &y);
     uint8_t seed[32] = {7};
     if (!rc) rc = zntt_random_elements(field, seed, (uint64_t*)x, (size_t)1 << L, nullptr);
+    uint64_t ninv[4];
+    n_inverse(field, L, ninv);
     for (int sh = 0; sh < kNumShapes && !rc; sh++) {
       const uint32_t lt = kShapes[sh].log_tile;
       TuneEntry best;
@@ -540,18 +542,23 @@ int zntt_autotune(int field, uint32_t log_n_min, uint32_t log_n_max) {
         if (plan.np == last_np && plan.p[0].k == last_k0) continue;  // same plan as a larger kmax
         last_np = plan.np;
         last_k0 = plan.p[0].k;
-        for (int w = 0; w < 2 && !rc; w++)
-          rc = run_plan(field, tw, plan, L, (const uint4*)x, (uint4*)y, nullptr, false, false, nullptr, st);
+        // Each repetition is a forward and an inverse transform (the inverse's
+        // last pass also scales by 1/n): one plan serves both directions.
+        auto both = [&]() {
+          int r2 = run_plan(field, tw, plan, L, (const uint4*)x, (uint4*)y, nullptr, false, false, nullptr, st);
+          if (!r2) r2 = run_plan(field, tw, plan, L, (const uint4*)x, (uint4*)y, nullptr, true, true, ninv, st);
+          return r2;
+        };
+        for (int w = 0; w < 2 && !rc; w++) rc = both();
         const int reps = L >= 22 ? 5 : L >= 18 ? 20 : 50;
         cudaEventRecord(e0, st);
-        for (int r = 0; r < reps && !rc; r++)
-          rc = run_plan(field, tw, plan, L, (const uint4*)x, (uint4*)y, nullptr, false, false, nullptr, st);
+        for (int r = 0; r < reps && !rc; r++) rc = both();
         cudaEventRecord(e1, st);
         cudaError_t ce = cudaEventSynchronize(e1);
         if (ce != cudaSuccess) rc = cuda_fail(ce, "autotune");
         float ms = 0;
         cudaEventElapsedTime(&ms, e0, e1);
-        const double us = 1e3 * ms / reps;
+        const double us = 1e3 * ms / (2 * reps);  // per transform, both directions averaged
         if (!rc && us < best.us) {
           best.field = field;
           best.log_n = L;
