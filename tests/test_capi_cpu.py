@@ -232,3 +232,24 @@ def test_batch_spin_limit_and_pool_stats_need_no_device(zntt):
     assert set(st) == {"acquires", "device_mallocs", "cached_bytes"}
     assert st["device_mallocs"] <= st["acquires"] * 2
     assert zntt.BATCH_SPIN_LIMIT == 1 << 22
+
+
+def test_shipped_tuning_table_covers_every_size_and_shape(zntt):
+    """The B200 table that bench.py loads has one entry per (field, log n, pass shape) for
+    both 256-bit fields and log n 10..24, each with a stage count its shape's tile can hold,
+    and it loads through zntt_tune_load (parsing needs no device)."""
+    import json
+    import os
+    path = os.path.join(os.path.dirname(zntt.__file__), "tune", "b200.json")
+    rows = json.load(open(path))
+    log_tile = {0: 11, 1: 10, 2: 9, 3: 8, 4: 9}  # kShapes in csrc/kernels.cuh
+    seen = {(r["field"], r["log_n"], r["shape"]) for r in rows}
+    for f in (0, 1):
+        for L in range(10, 25):
+            for sh, lt in log_tile.items():
+                assert (f, L, sh) in seen, (f, L, sh)
+    for r in rows:
+        assert r["gpu"] == "NVIDIA B200" and r["us"] > 0
+        assert 2 <= r["kmax"] <= log_tile[r["shape"]], r
+    assert zntt.lib().zntt_tune_load(path.encode()) == 0
+    zntt.tune_clear()
