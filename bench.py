@@ -509,9 +509,12 @@ def run_size_sweep(z, torch, stream, steps, warmup, peak_modmul, seed=66):
     """The single-transform configuration across sizes and directions: BN254-Fr 2^20, 2^22 and
     2^24, forward and inverse (nttWithTwiddles / inttWithTwiddles, libs/ntt/src/root.zig:148-212),
     and BLS12-381-Fr 2^24, with the tables resident.  Each entry: ms per transform, elements/s,
-    and the modmul rate ((n/2) log n products, plus n for the inverse's 1/n) over the live
-    multiply-pipe peak."""
+    the modmul rate ((n/2) log n products, plus n for the inverse's 1/n) over the live
+    multiply-pipe peak, and the algorithmic HBM rate (the vector read and written once,
+    2 n 32 bytes) over the measured copy bandwidth."""
     sptr = stream.cuda_stream
+    peaks, _ = measured_peaks()
+    hbm_peak = float(peaks["hbm_gbs"])
     out = {}
     for F, sizes in ((z.BN254_FR, (20, 22, 24)), (z.BLS12_381_FR, (24,))):
         x = torch.empty((1 << max(sizes)) * 4, dtype=torch.int64, device="cuda")
@@ -526,9 +529,11 @@ def run_size_sweep(z, torch, stream, steps, warmup, peak_modmul, seed=66):
                         run()
                     ms = time_region(torch, stream, run, steps) / steps
                     modmuls = n // 2 * L + (n if mode == z.INVERSE else 0)
+                    hbm_gbs = 2 * n * 32 / (ms * 1e-3) / 1e9
                     out[f"{F.name} 2^{L} {name}"] = {
                         "ms": ms, "elements_per_s": n / (ms * 1e-3), "modmul_per_s": modmuls / (ms * 1e-3),
-                        "frac": modmuls / (ms * 1e-3) / peak_modmul}
+                        "frac": modmuls / (ms * 1e-3) / peak_modmul, "hbm_gbs": hbm_gbs,
+                        "hbm_frac": hbm_gbs / hbm_peak}
         del x, y
     return out
 
