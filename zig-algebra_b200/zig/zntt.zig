@@ -57,18 +57,13 @@ fn fieldId(comptime F: type) c_int {
     }
 }
 
-var init_once = std.once(initDevice);
-var init_status: c_int = 0;
-
-fn initDevice() void {
-    init_status = zntt_init(0);
-}
-
 const DeviceFailure = error{ DeviceError, OutOfMemory };
 
+/// zntt_init is idempotent and thread-safe (a mutex inside the library): after
+/// the first call it only confirms that the library already runs on device 0,
+/// so every entry point calls it and the shim needs no once-guard of its own.
 fn ensureInit() DeviceFailure!void {
-    init_once.call();
-    if (init_status != 0) return error.DeviceError;
+    if (zntt_init(0) != 0) return error.DeviceError;
 }
 
 fn limbs(comptime F: type, data: []F) [*]u64 {
