@@ -416,3 +416,23 @@ def test_largest_order_transform(z):
     ks = [0, 1, n // 2 + 7, n - 1]
     pts = O.dft_points(F.id, _to_host(x), root, ks, workers=WORKERS)
     np.testing.assert_array_equal(_to_host(X)[ks], pts)
+
+
+def test_init_is_idempotent_and_keeps_its_device(z):
+    """The Zig shim calls zntt_init(0) on every entry point: a repeated call on the same device
+    returns OK at once, and a call naming another device is refused without disturbing the
+    library."""
+    L = z.lib()
+    assert L.zntt_init(0) == 0
+    assert L.zntt_init(0) == 0
+    with pytest.raises(z.ZnttError):
+        z._check(L.zntt_init(1))
+    assert L.zntt_init(0) == 0
+    root = z.primitiveRootOfUnity(z.BN254_FR, 10)
+    x = O.random_elements(O.BN254_FR, 91, 1 << 10)
+    want = x.copy()
+    st, tw = O.precompute_twiddles(O.BN254_FR, 10, root)
+    O.ntt_with_twiddles(O.BN254_FR, want, 10, tw, inverse=False, workers=1, inplace4=True)
+    got = x.copy()
+    z.ntt(z.BN254_FR, got, 10, root)
+    np.testing.assert_array_equal(got, want)
