@@ -116,28 +116,37 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
   const uint32_t xcols_log = pp.log_n - k;
   const uint64_t src_len = pp.src_len;
 
-  // ---- load: column-fastest, 16-byte halves ----
+  // ---- load: warp w stages the 128-element slices w, w + W, w + 2W, ... of
+  // the tile (DIT order), column-fastest in 16-byte halves.  These are the
+  // elements its radix-4 groups use while a group's span, 4 h C elements, stays
+  // within 128: those stage pairs exchange data only inside the warp and
+  // synchronise with __syncwarp instead of a CTA barrier (2^24: the load and
+  // three of the four stage pairs of every pass). ----
+  constexpr uint32_t W = THREADS / 32;
+  static_assert(TILE_MAX / THREADS >= 4, "each warp stages whole 128-element slices");
+  const uint32_t lane = tid & 31, warp = tid >> 5;
 #pragma unroll
-  for (uint32_t q = 0; q < 2 * TILE_MAX / THREADS; q++) {
-    const uint32_t idx = tid + q * THREADS;
-    if (FULL || idx < 2 * tile) {
-      const uint32_t h = idx & 1, e = idx >> 1, col = e & (C - 1), row = e >> c;
-      uint32_t g, t;
+  for (uint32_t r = 0; r < 2 * TILE_MAX / THREADS; r++) {
+    const uint32_t u = lane + 32 * (r & 7);
+    const uint32_t e = (warp + (r >> 3) * W) * 128 + (u >> 1), h = u & 1;
+    if (FULL || e < tile) {
+      const uint32_t col = e & (C - 1), t = e >> c;
+      uint32_t g;
       uint4 val;
       if (first) {
-        g = (row << xcols_log) + col0 + col;
-        t = rev_bits(row, k);
+        g = (rev_bits(t, k) << xcols_log) + col0 + col;
         if (EXT && g >= src_len) val = make_uint4(0, 0, 0, 0);
         else val = load_data<COHERENT>(pp.src + ((g << 1) | h));
       } else {
-        g = hi_base + (row << S) + m0 + col;
-        t = row;
+        g = hi_base + (t << S) + m0 + col;
         val = load_data<COHERENT>(pp.src + ((g << 1) | h));
       }
-      sm[h * TILE_MAX + ((t << c) | col)] = val;
+      sm[h * TILE_MAX + e] = val;
     }
   }
-  __syncthreads();
+  // A radix-4 pair whose h satisfies (h << (c + 2)) <= 128 is warp-local.
+  if (k >= 2 && (C << 2) <= 128u) __syncwarp();
+  else __syncthreads();
 
   // ---- radix-4 groups: stages i and i+1 on four elements in registers ----
   uint32_t i = 1;
@@ -184,7 +193,9 @@ __device__ __forceinline__ void ntt_tile(const PassParams& pp, uint64_t blk, uin
         sm_store<TILE_MAX>(sm, e0 + 3 * eh, x3);
       }
     }
-    __syncthreads();
+    // The next pair (stages i+2, i+3) is warp-local when its h = 2^(i+1) is.
+    if (i + 2 < k && ((2u << i) << (c + 2)) <= 128u) __syncwarp();
+    else __syncthreads();
   }
 
   // ---- an odd stage count ends with one radix-2 stage (stage k of the pass).
